@@ -1,0 +1,522 @@
+#!/usr/bin/env python
+"""Benchmark of the all-pole (LPC) filter on B200: fwd+bwd samples/s.
+
+One step = forward + backward of the filter over one batch of the workload,
+through the public API (``sample_wise_lpc`` then ``y.backward(grad_y)``, i.e.
+the gradients of sum(y * g) for x, A and zi).  Inputs are seeded synthetic
+signals with the workload's shapes and pole statistics (torchlpc_b200.synth).
+
+Default workload: B=8 signals, T=2^20 samples, order N=16 (8 pole pairs per
+512-sample frame, radius U[0.9, 0.999], zi ~ N(0,1)) — the long-sequence
+configuration the chunked scan targets.  ``--config`` selects another one.
+
+Prints ONE JSON line (rank 0).  ``--impl reference`` times the reference's own
+CPU implementation (DiffAPF/torchlpc's compiled operator and autograd, built
+into oracle/_ref) on the host cores instead.
+
+Multi-GPU (torchrun): every rank filters its own copy of the workload (signals
+are independent; there is no collective on the data path) -> weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from datetime import timedelta
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import torch  # noqa: E402
+import torch.distributed as dist  # noqa: E402
+
+METRIC = "fwd+bwd samples/s & % HBM peak, scan vs plain, at ≤1e-4 rel err vs FP64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg3", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
+    ap.add_argument("--algo", default="auto", choices=["auto", "plain", "chunked"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the per-config summary")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- utilities
+def rank_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rk = int(os.environ.get("RANK", "0"))
+    lr = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rk, lr
+
+
+def max_over_ranks(v: float, device) -> float:
+    if not dist.is_initialized():
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def bytes_per_sample(N: int, time_invariant: bool):
+    """Algorithmic HBM bytes per sample (fp32): fwd reads x, A and writes y;
+    bwd reads grad_y, A, y and writes grad_x, grad_A."""
+    if time_invariant:
+        return 8.0, 12.0
+    return 8.0 + 4.0 * N, 12.0 + 8.0 * N
+
+
+# --------------------------------------------------------------------------- workloads
+def load_workload(cfg: str, device, seed: int = 0):
+    from torchlpc_b200.synth import make_workload
+
+    return make_workload(cfg, seed=seed, device=device)
+
+
+def samples_of(w) -> int:
+    return int(w["S"]) if w["workload"].ragged else int(w["B"]) * int(w["T"])
+
+
+def coeff_arg(w, A):
+    """Coefficients as the public API takes them (time-invariant: expanded view)."""
+    if w["workload"].time_invariant:
+        return A[:, None, :].expand(-1, w["T"], -1)
+    return A
+
+
+# --------------------------------------------------------------------------- our arm
+def make_step(tl, w, x, A, zi, gy):
+    ragged = w["workload"].ragged
+
+    def step():
+        x.grad = A.grad = zi.grad = None
+        if ragged:
+            y = tl.sample_wise_lpc_ragged(x, A, w["offsets_dev"], zi)
+        else:
+            y = tl.sample_wise_lpc(x, coeff_arg(w, A), zi)
+        y.backward(gy)
+        return y
+
+    return step
+
+
+def count_kernels(fn) -> int:
+    from torch.profiler import ProfilerActivity, profile
+
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    n = 0
+    for e in prof.events():
+        if e.device_type.name == "CUDA" and "lpcb::" in e.name:
+            n += 1
+    return n
+
+
+def time_loop(fn, steps, warmup, device):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize(device)
+    if dist.is_initialized():
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        fn()
+    e.record()
+    torch.cuda.synchronize(device)
+    if dist.is_initialized():
+        dist.barrier()
+    return s.elapsed_time(e) / steps  # ms per step
+
+
+def kernel_times(tl, w, x, A, zi, gy, steps, device):
+    """Average device time of the forward and the fused backward operator
+    (CUDA events on the launching stream)."""
+    from torchlpc_b200 import _ops
+
+    Aa = coeff_arg(w, A).detach()
+    if w["workload"].time_invariant:
+        Aa = A.detach()
+    with torch.no_grad():
+        if w["workload"].ragged:
+            fwd = lambda: _ops.lpc_ragged(x.detach(), A.detach(), w["offsets_dev"], zi.detach())
+            y = fwd()
+            bwd = lambda: _ops.lpc_backward_ragged(gy, A.detach(), w["offsets_dev"], zi.detach(), y, True, True)
+        else:
+            fwd = lambda: _ops.lpc(x.detach(), Aa, zi.detach())
+            y = fwd()
+            bwd = lambda: _ops.lpc_backward(gy, Aa, zi.detach(), y, True, True)
+        tf = time_loop(fwd, steps, 3, device)
+        tb = time_loop(bwd, steps, 3, device)
+    return tf, tb
+
+
+def accuracy(tl, w, x, A, zi, gy, algo):
+    """Normwise max|out - ref| / max|ref| of y, zf and the three gradients of
+    the float32 path against the float64 sequential kernel on the same
+    (float32-rounded) inputs."""
+    def run(dt, al):
+        tl.set_algo(al)
+        xx = x.detach().to(dt).requires_grad_(True)
+        AA = A.detach().to(dt).requires_grad_(True)
+        zz = zi.detach().to(dt).requires_grad_(True)
+        if w["workload"].ragged:
+            y = tl.sample_wise_lpc_ragged(xx, AA, w["offsets_dev"], zz)
+            zf = None
+        else:
+            y, zf = tl.sample_wise_lpc(xx, coeff_arg(w, AA), zz, return_zf=True)
+        y.backward(gy.to(dt))
+        return {"y": y.detach(), "zf": None if zf is None else zf.detach(), "gx": xx.grad,
+                "gA": AA.grad, "gzi": zz.grad}
+
+    o32 = run(torch.float32, algo)
+    o64 = run(torch.float64, "plain")
+    tl.set_algo(algo)
+    out = {}
+    for k in o32:
+        if o32[k] is None:
+            continue
+        ref = o64[k]
+        den = ref.abs().max().item()
+        out[k] = (o32[k].double() - ref).abs().max().item() / (den if den > 0 else 1.0)
+    return out
+
+
+def e2e_time(tl, w, x_dev, A_dev, zi_dev, gy_dev, steps, warmup, device):
+    """The same step through the public API with HOST inputs: every step copies
+    x, A, zi, grad_y from pinned host memory and reads y and the three
+    gradients back into pinned host memory."""
+    hx, hA, hz, hg = (t.detach().cpu().pin_memory() for t in (x_dev, A_dev, zi_dev, gy_dev))
+    outs = {k: torch.empty(s, dtype=x_dev.dtype).pin_memory()
+            for k, s in (("y", x_dev.shape), ("gx", x_dev.shape), ("gA", A_dev.shape), ("gzi", zi_dev.shape))}
+    ragged = w["workload"].ragged
+
+    def step():
+        x = hx.to(device, non_blocking=True).requires_grad_(True)
+        A = hA.to(device, non_blocking=True).requires_grad_(True)
+        zi = hz.to(device, non_blocking=True).requires_grad_(True)
+        gy = hg.to(device, non_blocking=True)
+        if ragged:
+            y = tl.sample_wise_lpc_ragged(x, A, w["offsets_dev"], zi)
+        else:
+            y = tl.sample_wise_lpc(x, coeff_arg(w, A), zi)
+        y.backward(gy)
+        outs["y"].copy_(y.detach(), non_blocking=True)
+        outs["gx"].copy_(x.grad, non_blocking=True)
+        outs["gA"].copy_(A.grad, non_blocking=True)
+        outs["gzi"].copy_(zi.grad, non_blocking=True)
+
+    ms = time_loop(step, steps, warmup, device)
+    h2d = sum(t.numel() * t.element_size() for t in (hx, hA, hz, hg))
+    d2h = sum(t.numel() * t.element_size() for t in outs.values())
+    return ms, h2d, d2h
+
+
+def traffic_from_profiles(cfg: str, kernel: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        e = d.get(cfg, {}).get(kernel)
+        return None if e is None else float(e["bytes_per_launch"])
+    except (ValueError, KeyError, TypeError):
+        return None
+
+
+# --------------------------------------------------------------------------- reference (CPU)
+def reference_module():
+    from oracle.build import build_reference
+
+    path = build_reference()
+    if path is None:
+        return None, "reference CPU operator not built (oracle/_ref missing)"
+    sys.path.insert(0, str(path))
+    import warnings
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        import torchlpc  # the reference package, CPU operator compiled from its sources
+
+    if not torchlpc.EXTENSION_LOADED:
+        return None, "reference C++ extension failed to load"
+    return torchlpc, None
+
+
+def reference_sample(w, budget_signals=None):
+    """A bounded sample of the workload on the host: whole signals (dense: all
+    of B unless budget_signals; ragged: the first signals up to ~1/8 of the
+    samples, padded per the reference API, one signal per call)."""
+    wl = w["workload"]
+    if wl.ragged:
+        off = w["offsets"].cpu()
+        lens = (off[1:] - off[:-1]).tolist()
+        tot, picks = 0, []
+        for b, L in enumerate(lens):
+            picks.append(b)
+            tot += L
+            if tot >= samples_of(w) // 8:
+                break
+        return ("ragged", picks)
+    B = w["B"] if budget_signals is None else min(w["B"], budget_signals)
+    return ("dense", B)
+
+
+def reference_calls(ref, w):
+    """The reference CPU fwd+bwd (sample_wise_lpc + backward of sum(y*g)) over a
+    bounded sample of the workload.  Returns (run_once, samples, description)."""
+    wl = w["workload"]
+    x, A, zi, gy = (w[k].detach().cpu() for k in ("x", "A", "zi", "gy"))
+    kind, sel = reference_sample(w)
+    calls = []
+    if kind == "dense":
+        B = sel
+        T = w["T"]
+        if wl.time_invariant:
+            B = max(1, min(B, 64))  # the reference materialises (B,T,N) A; bound the host memory
+        calls.append((x[:B], A[:B], zi[:B], gy[:B]))
+        desc = f"{B} of {w['B']} signals x T={T}"
+        nsamp = B * T
+    else:
+        off = w["offsets"].cpu()
+        nsamp = 0
+        for b in sel:
+            s, e = int(off[b]), int(off[b + 1])
+            calls.append((x[None, s:e], A[None, s:e], zi[b:b + 1], gy[None, s:e]))
+            nsamp += e - s
+        desc = f"{len(sel)} of {w['B']} ragged signals ({nsamp} samples), one call per signal"
+
+    def once():
+        for xs, As, zs, gs in calls:
+            xx = xs.clone().requires_grad_(True)
+            AA = As.clone().requires_grad_(True)
+            zz = zs.clone().requires_grad_(True)
+            Ae = AA[:, None, :].expand(-1, xx.shape[1], -1) if wl.time_invariant else AA
+            y = ref.sample_wise_lpc(xx, Ae, zz)
+            y.backward(gs)
+
+    return once, nsamp, desc
+
+
+def time_reference(ref, w, seconds: float):
+    """Reference CPU fwd+bwd looped until `seconds` have elapsed (after one
+    warm-up pass); returns (samples/s, description, seconds per pass)."""
+    once, nsamp, desc = reference_calls(ref, w)
+    once()
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        once()
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or reps >= 50:
+            break
+    return nsamp * reps / el, desc, el / reps
+
+
+def run_reference(args):
+    ws, rk, lr = rank_info()
+    if rk != 0:
+        return 0
+    ref, why = reference_module()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return 0
+    device = "cuda" if torch.cuda.is_available() else "cpu"
+    w = load_workload(args.config, device)
+    once, nsamp, desc = reference_calls(ref, w)
+    for _ in range(max(1, args.warmup)):
+        once()
+    secs = []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        once()
+        secs.append(time.perf_counter() - t0)
+    per_step = sum(secs) / len(secs)
+    value = nsamp / per_step
+    threads = torch.get_num_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {w['workload'].note}", "sample": desc},
+        "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "reference",
+                         "sample": f"{desc}; reference torchlpc CPU operator (scan_cpu.cpp, OpenMP) + "
+                                   f"its autograd backward, fp32"},
+        "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------------------- main
+def run_ours(args):
+    ws, rk, lr = rank_info()
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    device = torch.device("cuda", lr)
+    torch.cuda.set_device(device)
+    import torchlpc_b200 as tl
+    from torchlpc_b200 import _ops
+
+    assert tl.EXTENSION_LOADED
+    tl.set_algo(args.algo)
+    w = load_workload(args.config, device, seed=rk)
+    if w["workload"].ragged:
+        w["offsets_dev"] = w["offsets"].to(device)
+    wl = w["workload"]
+    S = samples_of(w)
+    x = w["x"].requires_grad_(True)
+    A = w["A"].requires_grad_(True)
+    zi = w["zi"].requires_grad_(True)
+    gy = w["gy"]
+    step = make_step(tl, w, x, A, zi, gy)
+
+    launches_per_step = count_kernels(step)
+    sampler = ClockSampler(torch.cuda.current_device()) if rk == 0 else None
+    if sampler:
+        sampler.start()
+    ms = time_loop(step, args.steps, max(3, args.warmup), device)
+    clocks = sampler.stop() if sampler else None
+    ms = max_over_ranks(ms, device)
+    value = ws * S / (ms * 1e-3)
+
+    line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded; x, g ~ N(0,1); per-frame pole pairs interpolated per sample)",
+            "config": {"workload": f"{args.config}: {wl.note}", "B": w["B"], "T": w["T"], "N": w["N"],
+                       "samples_per_step": S, "algo": args.algo,
+                       "l2": "inputs larger than L2 (coefficients alone %.0f MiB)" % (
+                           A.numel() * A.element_size() / 2 ** 20),
+                       "parallelism": f"replicas x{ws} (independent signals, no collective)"},
+            "gpu_launches": launches_per_step * args.steps}
+    if clocks:
+        line["clocks"] = clocks
+
+    if rk == 0:
+        # roofline of the dominant kernel (forward or fused backward operator)
+        tf, tb = kernel_times(tl, w, x, A, zi, gy, max(5, args.steps // 2), device)
+        peak, peak_kind = measured_peaks()
+        bf, bb = bytes_per_sample(w["N"], wl.time_invariant)
+        kern, t_k, b_k = ("backward", tb, bb) if tb >= tf else ("forward", tf, bf)
+        achieved = S * b_k / (t_k * 1e-3) / 1e9
+        tr = traffic_from_profiles(args.config, kern)
+        line["roofline"] = {"bound": "hbm", "kernel": f"fused {kern} operator", "achieved": achieved,
+                            "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                            "peak_source": peak_kind, "traffic": tr,
+                            "algorithmic_bytes_per_launch": S * b_k, "launch_ms": t_k}
+        step_bytes = S * (bf + bb)
+        line["hbm_frac_fwd_bwd"] = step_bytes / (ms * 1e-3) / 1e9 / peak
+        line["kernel_ms"] = {"forward": tf, "backward": tb}
+        # scan vs plain on the same GPU
+        if args.algo != "plain" and "chunked" in tl.available_algos():
+            tl.set_algo("plain")
+            msp = time_loop(step, max(2, args.steps // 4), 1, device)
+            tl.set_algo(args.algo)
+            line["plain"] = {"value": S / (msp * 1e-3), "ms_per_step": msp,
+                             "speedup": msp / ms}
+        line["max_rel_err_vs_fp64"] = accuracy(tl, w, x, A, zi, gy, args.algo)
+        if not args.no_e2e:
+            ems, h2d, d2h = e2e_time(tl, w, x, A, zi, gy, max(3, args.steps // 4), 2, device)
+            line["e2e"] = {"value": S / (ems * 1e-3), "unit": "samples/s", "ms_per_step": ems,
+                           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        if ws == 1 and not args.no_cpu_baseline:
+            ref, why = reference_module()
+            if ref is not None:
+                v, desc, _ = time_reference(ref, w, args.cpu_seconds)
+                line["cpu_baseline"] = {"value": v, "unit": "samples/s", "cores": torch.get_num_threads(),
+                                        "kind": "reference",
+                                        "sample": f"{desc}; reference torchlpc CPU operator + autograd, fp32, "
+                                                  f"looped for ~{args.cpu_seconds:.0f} s"}
+            else:
+                line["cpu_baseline"] = {"value": None, "unavailable": why}
+        print(json.dumps(line), flush=True)
+    if dist.is_initialized():
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,119 @@
+/*
+ * lpc_b200 — C ABI of the B200 (sm_100a) time-varying all-pole filter.
+ *
+ *   y[b,t] = x[b,t] - sum_{i<N} A[b,t,i] * y[b,t-i-1],   y[b,-k-1] = zi[b,k]
+ *
+ * Plain pointers and sizes only (no torch types).  All pointers are DEVICE
+ * pointers on the current CUDA device unless stated otherwise; every entry
+ * point is asynchronous on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and returns an lpc_status code.  No entry point allocates memory:
+ * callers pass a workspace of at least the size the matching *_workspace_size
+ * query returns (0 bytes is valid when that query returns 0).
+ *
+ * Element type: `dtype` is LPC_F32 (float) or LPC_F64 (double) for every
+ * floating-point buffer of a call.
+ *
+ * Coefficient addressing (strides in elements, the last dimension is unit
+ * stride):  A[b,t,i] = A[b*a_stride_b + t*a_stride_t + i].  a_stride_t == 0
+ * is a time-invariant filter (a (B,N) tensor broadcast over T, e.g.
+ * A[:,None,:].expand(-1,T,-1)); its coefficient gradient is then the (B,N)
+ * sum over T.  x, y, grad_y, grad_x are dense (B,T) row-major; zi, grad_zi
+ * are dense (B,N).
+ */
+#ifndef LPC_B200_H
+#define LPC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum lpc_status {
+    LPC_OK = 0,
+    LPC_ERR_INVALID_ARGUMENT = 1, /* bad size, stride, dtype or NULL pointer     */
+    LPC_ERR_UNSUPPORTED = 2,      /* valid request this build cannot serve        */
+    LPC_ERR_WORKSPACE = 3,        /* workspace missing or smaller than required   */
+    LPC_ERR_CUDA = 4,             /* a CUDA runtime call failed (launch, memset)  */
+    LPC_ERR_TIMEOUT = 5           /* a bounded device-side wait gave up           */
+};
+
+enum lpc_dtype { LPC_F32 = 0, LPC_F64 = 1 };
+
+/* Algorithm selection for the forward/backward passes. */
+enum lpc_algo {
+    LPC_ALGO_AUTO = 0,    /* choose by (B, T, N) and the device's SM count          */
+    LPC_ALGO_PLAIN = 1,   /* one warp per signal, sequential in time               */
+    LPC_ALGO_CHUNKED = 2  /* chunked linear-recurrence scan, parallel in time      */
+};
+
+/* Human-readable text for a status code (static storage). */
+const char *lpc_b200_status_string(int status);
+
+/* ABI version of this library (major*10000 + minor*100 + patch). */
+int lpc_b200_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Forward filter.
+ * Replaces the reference operator torchlpc::lpc(x, A, zi) -> y
+ *   (torchlpc/csrc/scan_cpu.cpp:143-164 CPU, torchlpc/csrc/cuda/lpc.cu:115-175
+ *    CUDA; schema scan_cpu.cpp:169), called from LPC.forward (core.py:161-163).
+ * zi may be NULL (zero initial conditions).  y must not alias x.
+ * ------------------------------------------------------------------------- */
+size_t lpc_b200_forward_workspace_size(int dtype, int algo, int64_t B, int64_t T,
+                                       int64_t N, int64_t a_stride_t);
+
+int lpc_b200_forward(int dtype, int algo, const void *x, const void *A,
+                     const void *zi, void *y, int64_t B, int64_t T, int64_t N,
+                     int64_t a_stride_b, int64_t a_stride_t, void *workspace,
+                     size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Fused backward: grad_x, grad_A and grad_zi of the loss given grad_y, in one
+ * pass over time (reversed filter with the diagonally shifted coefficients
+ * A[t+i+1,i]; grad_A[t,i] = -grad_x[t]*y[t-i-1] fused into the epilogue).
+ * Replaces LPC.backward (torchlpc/core.py:186-229).
+ * y is the forward output saved for backward.  grad_A is (B,T,N) dense, or
+ * (B,N) when a_stride_t == 0.  grad_A and grad_zi may be NULL (not wanted);
+ * grad_x is always written.  zi may be NULL (zero initial conditions).
+ * ------------------------------------------------------------------------- */
+size_t lpc_b200_backward_workspace_size(int dtype, int algo, int64_t B, int64_t T,
+                                        int64_t N, int64_t a_stride_t);
+
+int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A,
+                      const void *zi, const void *y, void *grad_x, void *grad_A,
+                      void *grad_zi, int64_t B, int64_t T, int64_t N,
+                      int64_t a_stride_b, int64_t a_stride_t, void *workspace,
+                      size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Order-1 recurrence  out[t] = decay[t]*out[t-1] + impulse[t],  out[-1]=init.
+ * Replaces the reference operator torchlpc::scan(impulse, decay, init)
+ *   (torchlpc/csrc/scan_cpu.cpp:28-78,124-141; linear_recurrence.cu:232-291;
+ *    schema scan_cpu.cpp:168), called from Recurrence (recurrence.py:45-84).
+ * init may be NULL (zero).
+ * ------------------------------------------------------------------------- */
+size_t lpc_b200_scan_workspace_size(int dtype, int algo, int64_t B, int64_t T);
+
+int lpc_b200_scan(int dtype, int algo, const void *impulse, const void *decay,
+                  const void *init, void *out, int64_t B, int64_t T,
+                  void *workspace, size_t workspace_bytes, void *stream);
+
+/* Gradients of the order-1 recurrence (replaces Recurrence.backward,
+ * torchlpc/recurrence.py:92-126): grad_impulse[t] = grad_out[t] +
+ * decay[t+1]*grad_impulse[t+1]; grad_decay[t] = grad_impulse[t]*out[t-1];
+ * grad_init = decay[0]*grad_impulse[0].  grad_decay/grad_init may be NULL. */
+size_t lpc_b200_scan_backward_workspace_size(int dtype, int algo, int64_t B, int64_t T);
+
+int lpc_b200_scan_backward(int dtype, int algo, const void *grad_out,
+                           const void *decay, const void *init, const void *out,
+                           void *grad_impulse, void *grad_decay, void *grad_init,
+                           int64_t B, int64_t T, void *workspace,
+                           size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LPC_B200_H */

@@ -1,0 +1,99 @@
+"""torchlpc_b200 — B200-native (sm_100a) differentiable time-varying all-pole filter.
+
+Drop-in for the ``sample_wise_lpc`` / ``linear_recurrence`` path of
+DiffAPF/torchlpc (torchlpc/__init__.py:28-104): same functions, argument
+meaning, shapes and error behaviour, computed by hand-written CUDA kernels
+behind the C ABI of ``liblpc_b200`` (include/lpc_b200.h).  CUDA tensors only;
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+from typing import Optional, Tuple, Union
+
+import torch
+
+from ._ops import EXTENSION_LOADED, available_algos, get_algo, set_algo
+from .core import LPC
+from .recurrence import Recurrence
+
+__all__ = ["sample_wise_lpc", "linear_recurrence", "LPC", "Recurrence", "EXTENSION_LOADED",
+           "set_algo", "get_algo", "available_algos"]
+
+
+def linear_recurrence(a: torch.Tensor, x: torch.Tensor, zi: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """y[n] = x[n] + a[n] * y[n-1], y[-1] = zi (torchlpc/__init__.py:31-60).
+
+    Shapes: a (B,T), x (B,T), zi (B,) (defaults to zeros).
+    """
+    assert a.shape == x.shape
+    assert a.ndim == 2
+    assert x.ndim == 2
+    B, _ = a.shape
+    if zi is None:
+        zi = a.new_zeros(B)
+    else:
+        assert zi.shape == (B,)
+    return Recurrence.apply(a, x, zi)  # type: ignore
+
+
+def _time_invariant_source(a: torch.Tensor) -> Optional[torch.Tensor]:
+    """For coefficients broadcast over time (stride 0 along T, e.g.
+    ``a0[:, None, :].expand(-1, T, -1)``) return the (B, N) tensor they view, so
+    that the fused time-invariant kernels run and the coefficient gradient
+    reaches ``a0`` as a (B, N) reduction instead of a materialised (B, T, N)
+    tensor.  Returns None when the pattern is not recognised."""
+    try:
+        if a.dim() != 3 or a.shape[1] <= 1 or a.stride(1) != 0:
+            return None
+        if torch._C._functorch.is_functorch_wrapped_tensor(a):
+            return None
+        B, _, N = a.shape
+        if not a.requires_grad:
+            return a[:, 0, :]
+        base = a._base
+        if base is None or base.data_ptr() != a.data_ptr():
+            return None
+        if base.shape == (B, N) and (B == 1 or base.stride(0) == a.stride(0)) and \
+                (N == 1 or base.stride(1) == a.stride(2)):
+            return base
+        if base.shape == (B, 1, N) and (B == 1 or base.stride(0) == a.stride(0)) and \
+                (N == 1 or base.stride(2) == a.stride(2)):
+            return base.squeeze(1)
+    except (RuntimeError, AttributeError):
+        return None
+    return None
+
+
+def sample_wise_lpc(
+    x: torch.Tensor,
+    a: torch.Tensor,
+    zi: Optional[torch.Tensor] = None,
+    return_zf: bool = False,
+) -> Union[torch.Tensor, Tuple[torch.Tensor, torch.Tensor]]:
+    """Sample-wise all-pole (LPC) filtering (torchlpc/__init__.py:63-104).
+
+    y[b,t] = x[b,t] - sum_{i=1..N} a[b,t,i-1] * y[b,t-i], with zi[b,k] = y[b,-1-k].
+
+    Shapes: x (B,T), a (B,T,N), zi (B,N) (defaults to zeros).  Returns y (B,T),
+    and with ``return_zf`` also the final delay values ``y[:, -N:].flip(1)``.
+    """
+    assert x.shape[0] == a.shape[0]
+    assert x.shape[1] == a.shape[1]
+    assert x.ndim == 2
+    assert a.ndim == 3
+
+    B, T, order = a.shape
+    if zi is None:
+        zi = a.new_zeros(B, order)
+    else:
+        assert zi.shape == (B, order)
+
+    if order == 1:
+        y = linear_recurrence(-a.squeeze(2), x, zi.squeeze(1))
+    else:
+        src = _time_invariant_source(a)
+        y = LPC.apply(x, src if src is not None else a, zi)
+
+    if return_zf:
+        return y, y[:, -order:].flip(1)
+    return y

@@ -1,0 +1,96 @@
+"""``LPC``: the all-pole filter as a torch.autograd.Function.
+
+Interface and semantics follow torchlpc.core.LPC (torchlpc/core.py:159-265):
+``LPC.apply(x, A, zi)`` with x (B,T), A (B,T,N), zi (B,N); it saves (A, zi, y)
+for backward and forward-mode AD, defines ``jvp`` and ``vmap``.  As an
+extension, A may also be a time-invariant (B,N) tensor.
+
+Backward: one fused CUDA kernel produces grad_x, grad_A and grad_zi
+(``torch.ops.torchlpc_b200.lpc_backward``).  When a graph of the backward is
+requested (``create_graph=True``, e.g. gradgradcheck) the backward is instead
+composed from differentiable pieces around ``LPC.apply`` itself: the reversed
+filter over the coefficient diagonal A[t+1+i, i], gathered from a
+time-padded A.
+"""
+from __future__ import annotations
+
+from typing import Any, List, Optional, Tuple
+
+import torch
+import torch.nn.functional as F
+from torch.autograd import Function
+
+from . import _ops
+
+
+def _lagged_outputs(y: torch.Tensor, zi: torch.Tensor, order: int) -> torch.Tensor:
+    """(B,T,N) with [b,t,i] = y[b,t-1-i] (zi[b,k] standing for y[b,-1-k])."""
+    return torch.cat([zi.flip(1), y[:, :-1]], dim=1).unfold(1, order, 1).flip(2)
+
+
+def _composed_backward(grad_y, A, zi, y, needs):
+    """Differentiable backward (used only when create_graph=True)."""
+    B, T = grad_y.shape
+    order = A.shape[-1]
+    A3 = A[:, None, :].expand(B, T, order) if A.dim() == 2 else A
+    # D[t', i] = A[t'-N+1+i, i] for t' = 0..T+N-1 (t = t'-N), zero outside [0, T)
+    A_pad = F.pad(A3, (0, 0, order, order + 1))
+    tp = torch.arange(T + order, device=A.device)
+    idx = (tp[:, None] + 1 + torch.arange(order, device=A.device)[None, :])
+    D = A_pad.gather(1, idx[None].expand(B, -1, -1))
+    gy_ext = F.pad(grad_y, (order, 0))
+    u = LPC.apply(gy_ext.flip(1), D.flip(1).conj_physical(), torch.zeros_like(zi))
+    gx_ext = u.flip(1)
+    grad_x = gx_ext[:, order:] if needs[0] else None
+    grad_zi = gx_ext[:, :order].flip(1) if needs[2] else None
+    grad_A = None
+    if needs[1]:
+        gA = -_lagged_outputs(y, zi, order).conj_physical() * gx_ext[:, order:].unsqueeze(2)
+        grad_A = gA.sum(1) if A.dim() == 2 else gA
+    return grad_x, grad_A, grad_zi
+
+
+class LPC(Function):
+    @staticmethod
+    def forward(x: torch.Tensor, A: torch.Tensor, zi: torch.Tensor) -> torch.Tensor:
+        return _ops.lpc(x, A, zi)
+
+    @staticmethod
+    def setup_context(ctx: Any, inputs: List[Any], output: Any) -> Any:
+        _, A, zi = inputs
+        y = output
+        ctx.save_for_backward(A, zi, y)
+        ctx.save_for_forward(A, zi, y)
+
+    @staticmethod
+    def backward(ctx: Any, grad_y: torch.Tensor
+                 ) -> Tuple[Optional[torch.Tensor], Optional[torch.Tensor], Optional[torch.Tensor]]:
+        A, zi, y = ctx.saved_tensors
+        needs = ctx.needs_input_grad
+        if torch.is_grad_enabled():
+            return _composed_backward(grad_y, A, zi, y, needs)
+        gx, gA, gzi = _ops.lpc_backward(grad_y, A, zi, y, bool(needs[1]), bool(needs[2]))
+        return (gx if needs[0] else None, gA if needs[1] else None, gzi if needs[2] else None)
+
+    @staticmethod
+    def jvp(ctx: Any, grad_x: torch.Tensor, grad_A: torch.Tensor, grad_zi: torch.Tensor) -> torch.Tensor:
+        A, zi, y = ctx.saved_tensors
+        order = A.shape[-1]
+        fwd_zi = grad_zi if grad_zi is not None else torch.zeros_like(zi)
+        fwd_x = grad_x if grad_x is not None else torch.zeros_like(y)
+        if grad_A is not None:
+            lagged = _lagged_outputs(y, zi, order)
+            dA = grad_A[:, None, :] if grad_A.dim() == 2 else grad_A
+            fwd_x = fwd_x - torch.sum(lagged * dA, dim=2)
+        return LPC.apply(fwd_x, A, fwd_zi)
+
+    @staticmethod
+    def vmap(info, in_dims, *args):
+        def front(t, bdim):
+            if bdim is None:
+                return t.expand(info.batch_size, *t.shape)
+            return t.movedim(bdim, 0)
+
+        x, A, zi = (t.reshape(-1, *t.shape[2:]) for t in map(front, args, in_dims))
+        y = LPC.apply(x, A, zi)
+        return y.reshape(info.batch_size, -1, *y.shape[1:]), 0

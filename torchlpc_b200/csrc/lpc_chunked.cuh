@@ -1,0 +1,24 @@
+// Chunked linear-recurrence scan kernels (parallel in time).
+#pragma once
+
+#include "lpc_plain.cuh"
+
+namespace lpcb {
+
+// Largest filter order any entry point accepts (the reference's limit,
+// torchlpc/csrc/cuda/lpc.cu:135).
+constexpr int64_t kMaxOrder = 1024;
+
+bool chunked_supported(int64_t N);
+bool chunked_preferred(int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
+size_t chunked_forward_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
+size_t chunked_backward_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
+
+template <typename T>
+cudaError_t chunked_forward(const FwdArgs<T> &p, bool neg, void *ws, size_t ws_bytes,
+                            cudaStream_t st);
+template <typename T>
+cudaError_t chunked_backward(const BwdArgs<T> &p, bool neg, void *ws, size_t ws_bytes,
+                             cudaStream_t st);
+
+}  // namespace lpcb
