@@ -46,6 +46,7 @@ enum lpc_algo {
     LPC_ALGO_AUTO = 0,    /* choose by (B, T, N) and the device's SM count          */
     LPC_ALGO_PLAIN = 1,   /* one warp per signal, sequential in time               */
     LPC_ALGO_CHUNKED = 2  /* chunked linear-recurrence scan, parallel in time      */
+                          /* (orders above 32 run the plain kernels)             */
 };
 
 /* Human-readable text for a status code (static storage). */

@@ -33,7 +33,7 @@ def p(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
 
 
-@pytest.mark.parametrize("algo", [1])
+@pytest.mark.parametrize("algo", [1, 2])
 def test_forward_backward_through_c_abi(lib, algo):
     w = make_workload("cfg2", seed=3, B=4, T=3000)
     x, A, zi, gy = (w[k].cuda() for k in ("x", "A", "zi", "gy"))

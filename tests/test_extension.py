@@ -11,7 +11,7 @@ from tests.test_grad import create_test_inputs
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("algo", [1])
+@pytest.mark.parametrize("algo", [1, 2])
 @pytest.mark.parametrize("samples", [64, 4097])
 def test_scan_equiv(samples, algo):
     g = torch.Generator().manual_seed(samples)
@@ -23,7 +23,7 @@ def test_scan_equiv(samples, algo):
     assert np.allclose(out.cpu().double().numpy(), ref, atol=5e-6)
 
 
-@pytest.mark.parametrize("algo", [1])
+@pytest.mark.parametrize("algo", [1, 2])
 @pytest.mark.parametrize("samples", [1021, 4097])
 def test_lpc_equiv(samples, algo):
     x, A, zi = create_test_inputs(4, samples, seed=samples)

@@ -34,7 +34,7 @@ def create_test_inputs(batch_size, samples, seed=0):
     return x, A, zi
 
 
-@pytest.fixture(params=["plain"])
+@pytest.fixture(params=["plain", "chunked"])
 def algo(request):
     old = tl.get_algo()
     tl.set_algo(request.param)

@@ -15,7 +15,7 @@ from tests.gpu_helpers import TOL32, TOL64, err, oracle_fwd_bwd, run_fwd_bwd, to
 
 pytestmark = pytest.mark.gpu
 
-ALGOS = ["plain"]
+ALGOS = ["plain", "chunked"]
 CASES = [n for n in golden_names() if not n.startswith("scan") and "ragged" not in n]
 
 

@@ -14,7 +14,7 @@ from tests.test_grad import create_test_inputs
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("algo", ["plain"])
+@pytest.mark.parametrize("algo", ["plain", "chunked"])
 def test_vmap(algo):
     tl.set_algo(algo)
     try:
@@ -39,7 +39,7 @@ def test_vmap(algo):
         tl.set_algo("auto")
 
 
-@pytest.mark.parametrize("algo", ["plain"])
+@pytest.mark.parametrize("algo", ["plain", "chunked"])
 def test_parallel_scan_vmap(algo):
     tl.set_algo(algo)
     try:

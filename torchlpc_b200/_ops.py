@@ -38,7 +38,7 @@ def available_algos():
     return ["plain", "chunked"] if _CHUNKED else ["plain"]
 
 
-_CHUNKED = False
+_CHUNKED = True
 
 
 def _require():

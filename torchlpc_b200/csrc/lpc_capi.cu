@@ -20,8 +20,11 @@ bool sizes_ok(int64_t B, int64_t T, int64_t N) {
 }
 
 // Choice between the sequential and the chunked kernels.
+// LPC_ALGO_CHUNKED falls back to the plain kernels for orders the chunked
+// kernels do not cover (N > 32).
 int resolve_algo(int algo, int64_t B, int64_t T, int64_t N, int64_t a_stride_t) {
-    if (algo == LPC_ALGO_PLAIN || algo == LPC_ALGO_CHUNKED) return algo;
+    if (algo == LPC_ALGO_PLAIN) return algo;
+    if (algo == LPC_ALGO_CHUNKED) return chunked_supported(N) ? algo : LPC_ALGO_PLAIN;
     return chunked_preferred(B, T, N, a_stride_t) ? LPC_ALGO_CHUNKED : LPC_ALGO_PLAIN;
 }
 
@@ -33,7 +36,6 @@ int forward_t(int algo, const void *x, const void *A, const void *zi, void *y, i
                  static_cast<T *>(y), B, T_, N, sb, st};
     if (B == 0 || T_ == 0) return LPC_OK;
     if (algo == LPC_ALGO_CHUNKED) {
-        if (!chunked_supported(N)) return LPC_ERR_UNSUPPORTED;
         if (ws_bytes < chunked_forward_workspace(sizeof(T), B, T_, N, st)) return LPC_ERR_WORKSPACE;
         return cuda_status(chunked_forward<T>(p, false, ws, ws_bytes, stream));
     }
@@ -54,7 +56,6 @@ int backward_t(int algo, const void *gy, const void *A, const void *zi, const vo
         return cuda_status(cudaGetLastError());
     }
     if (algo == LPC_ALGO_CHUNKED) {
-        if (!chunked_supported(N)) return LPC_ERR_UNSUPPORTED;
         if (ws_bytes < chunked_backward_workspace(sizeof(T), B, T_, N, st)) return LPC_ERR_WORKSPACE;
         return cuda_status(chunked_backward<T>(p, false, ws, ws_bytes, stream));
     }
