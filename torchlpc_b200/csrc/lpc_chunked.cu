@@ -102,6 +102,18 @@ struct Cfg {
     static constexpr int W = NP * ((16 + NP - 1) / NP);  // steps per window, multiple of NP
 };
 
+// Per-chunk stride of a coefficient window in shared memory: W rows of NP plus
+// one 16-byte pad so that the rows different chunks read in the same step
+// fall in different banks.
+__host__ __device__ constexpr int group_stride(int W, int NP, int esz) { return W * NP + 16 / esz; }
+// Row stride of a stored affine map (16-byte aligned, padded against bank conflicts).
+__host__ __device__ constexpr int map_row_stride(int NP, int esz) {
+    return ((NP + 16 / esz - 1) / (16 / esz)) * (16 / esz) + 16 / esz;
+}
+__host__ __device__ constexpr int map_stride(int NP, int esz) {
+    return NP * map_row_stride(NP, esz) + ((NP + 16 / esz - 1) / (16 / esz)) * (16 / esz);
+}
+
 // acc - sum_i a[i] * h[(u-1-i) mod NP] with two partial chains (even/odd taps)
 // and the newest tap (i = 0) applied last, so consecutive steps overlap and
 // the loop-carried path is one FMA.
@@ -143,35 +155,33 @@ __device__ __forceinline__ void lds_row(T (&dst)[NP], const T *src) {
 
 // Shared-memory plan (bytes), all regions 16-byte aligned.
 struct SmemPlan {
-    size_t abuf, ibuf, obuf, ybuf, maps, tmp, ent, sin, misc, total;
+    size_t abuf, ibuf, obuf, ybuf, maps, st, sin, misc, total;
     __host__ __device__ SmemPlan(size_t esz, int NP, int W, int G, int N, bool rev) {
         auto al = [](size_t v) { return (v + 15) & ~size_t(15); };
         size_t off = 0;
         abuf = off;
-        const size_t abytes = al((size_t)2 * G * W * NP * esz);
-        // the tree maps and their scratch alias the window buffers (phase B
-        // runs between the window loops of phases A and D)
+        const size_t abytes = al((size_t)2 * G * group_stride(W, NP, (int)esz) * esz);
+        // the tree maps alias the window buffers (phases B/C run between the
+        // window loops of phases A and D)
         int Gp = 1;
         while (Gp < G) Gp <<= 1;
-        const size_t mapbytes = al((size_t)Gp * (N * N + N) * esz);
-        const size_t tmpbytes = al((size_t)(Gp / 2 > 0 ? Gp / 2 : 1) * (N * N + N) * esz);
-        const size_t region = abytes > mapbytes + tmpbytes ? abytes : mapbytes + tmpbytes;
+        const size_t mapbytes = al((size_t)Gp * map_stride(NP, (int)esz) * esz);
         maps = off;
-        tmp = off + mapbytes;
-        off += al(region);
+        off += al(abytes > mapbytes ? abytes : mapbytes);
         ibuf = off;
         off += al((size_t)2 * G * W * esz);
         obuf = off;
         off += al((size_t)G * W * esz);
         ybuf = off;
         if (rev) off += al((size_t)2 * G * (W + NP) * esz);
-        ent = off;
-        off += al((size_t)G * N * esz);
+        st = off;  // FP64 entry states of the tree nodes
+        off += al((size_t)Gp * NP * sizeof(double));
         sin = off;
-        off += al((size_t)N * 2 * sizeof(double));
+        off += al((size_t)NP * sizeof(double));
         misc = off;
         off += 64;
         total = off;
+        (void)N;
     }
 };
 
@@ -190,6 +200,7 @@ struct Loader {
     static constexpr int W = Cfg<NP>::W;
     static constexpr int THREADS = Cfg<NP>::THREADS;
     static constexpr int V = 16 / sizeof(T);
+    static constexpr int GS = group_stride(W, NP, sizeof(T));
 
     // Vector fast path: order equals the padded order, rows are dense and
     // 16-byte aligned, so every index below divides by a compile-time constant.
@@ -211,7 +222,7 @@ struct Loader {
                     const int g = e / VPW;
                     const int v = e - g * VPW;
                     const int64_t t0 = tb + (int64_t)g * p.L + (int64_t)w * W;
-                    T *dst = As + (size_t)g * W * NP + v * V;
+                    T *dst = As + (size_t)g * GS + v * V;
                     const T *src = Ab + t0 * NP + v * V;
                     if (t0 + W <= p.T) {
                         cp_async<16>(dst, src);
@@ -234,7 +245,7 @@ struct Loader {
                     const int r = rem / N;
                     const int i = rem - r * N;
                     const int64_t t = tb + (int64_t)g * p.L + (int64_t)w * W + r;
-                    T *dst = As + ((size_t)g * W + r) * NP + i;
+                    T *dst = As + (size_t)g * GS + r * NP + i;
                     if (t < p.T)
                         cp_async<sizeof(T)>(dst, Ab + t * p.as_t + i);
                     else
@@ -263,7 +274,7 @@ struct Loader {
                     const int i0 = (rem - q * RV) * V;
                     const int64_t top = p.T - (tb + (int64_t)g * p.L + (int64_t)w * W);
                     const int64_t r = top - (W - 1) + q;
-                    T *Ag = As + (size_t)g * W * NP;
+                    T *Ag = As + (size_t)g * GS;
                     const bool in_range = (r >= 0 && r < p.T);
                     const T *src = Ab + r * NP + i0;
 #pragma unroll
@@ -289,7 +300,7 @@ struct Loader {
                     const int64_t r = top - (W - 1) + q;
                     const int s = (int)(top - r) + i;
                     if (s < 0 || s >= W) continue;
-                    T *dst = As + ((size_t)g * W + s) * NP + i;
+                    T *dst = As + (size_t)g * GS + s * NP + i;
                     if (r >= 0 && r < p.T)
                         cp_async<sizeof(T)>(dst, Ab + r * p.as_t + i);
                     else
@@ -335,6 +346,10 @@ template <typename T, int NP, bool REV, bool NEG>
 __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chunked_kernel(ChunkParams<T> p) {
     constexpr int W = Cfg<NP>::W;
     constexpr int THREADS = Cfg<NP>::THREADS;
+    constexpr int V = 16 / sizeof(T);
+    constexpr int GS = group_stride(W, NP, sizeof(T));
+    constexpr int RS = map_row_stride(NP, sizeof(T));
+    constexpr int MS = map_stride(NP, sizeof(T));
     extern __shared__ __align__(16) unsigned char smem[];
     const int N = p.N;
     const int G = p.G;
@@ -344,20 +359,17 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
     T *ibuf = reinterpret_cast<T *>(smem + S.ibuf);
     T *obuf = reinterpret_cast<T *>(smem + S.obuf);
     T *ybuf = reinterpret_cast<T *>(smem + S.ybuf);
-    T *maps = reinterpret_cast<T *>(smem + S.maps);  // [Gp][N*N + N]: P (row-major) then z
-    T *tmpm = reinterpret_cast<T *>(smem + S.tmp);
-    T *ent = reinterpret_cast<T *>(smem + S.ent);    // [G][N] entry states
-    double *sin_d = reinterpret_cast<double *>(smem + S.sin);  // [2][N]
+    T *maps = reinterpret_cast<T *>(smem + S.maps);  // [Gp][NP rows of RS | z]
+    double *st = reinterpret_cast<double *>(smem + S.st);      // [Gp][NP]
+    double *s_in = reinterpret_cast<double *>(smem + S.sin);   // [NP]
     int64_t *misc = reinterpret_cast<int64_t *>(smem + S.misc);
-    const int MS = N * N + N;  // map stride
     int Gp = 1;
     while (Gp < G) Gp <<= 1;
 
     const bool vec = Loader<T, NP, REV>::fast(p);
     const int grp = tid / (N + 1);
     const int kk = tid - grp * (N + 1);
-    const int steps_per_chunk = p.L;
-    const int nwin = steps_per_chunk / W;
+    const int nwin = p.L / W;
 
     for (;;) {
         __syncthreads();
@@ -372,10 +384,10 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
         const int Gb = (int)min64(G, (rem + p.L - 1) / p.L);
 
         // ------------------------------------------------------------ phase A
-        // padded coefficient columns must read as zero
-        if (N < NP)
-            for (int e = tid; e < 2 * G * W * NP; e += THREADS)
-                if (e % NP >= N) Abuf[e] = T(0);
+        // chunk maps: N basis filters + one zero-state filter per chunk
+        if (N < NP)  // padded coefficient columns must read as zero
+            for (int e = tid; e < 2 * G * GS; e += THREADS)
+                if ((e % GS) % NP >= N) Abuf[e] = T(0);
         const bool active = grp < Gb;
         const bool xlane = (kk == N);
         T h[NP];
@@ -385,16 +397,16 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
         Loader<T, NP, REV>::load(p, vec, b, tb, Gb, 0, Abuf, ibuf, nullptr, false);
         cp_async_commit();
         for (int w = 0; w < nwin; ++w) {
-            T *As = Abuf + (size_t)(w & 1) * G * W * NP;
-            T *xs = ibuf + (size_t)(w & 1) * G * W;
+            const T *As = Abuf + (size_t)(w & 1) * G * GS;
+            const T *xs = ibuf + (size_t)(w & 1) * G * W;
             if (w + 1 < nwin)
-                Loader<T, NP, REV>::load(p, vec, b, tb, Gb, w + 1, Abuf + (size_t)((w + 1) & 1) * G * W * NP,
+                Loader<T, NP, REV>::load(p, vec, b, tb, Gb, w + 1, Abuf + (size_t)((w + 1) & 1) * G * GS,
                                          ibuf + (size_t)((w + 1) & 1) * G * W, nullptr, false);
             cp_async_commit();
             cp_async_wait<1>();
             __syncthreads();
             if (active) {
-                const T *Ag = As + (size_t)grp * W * NP;
+                const T *Ag = As + (size_t)grp * GS;
                 const T *xg = xs + (size_t)grp * W;
 #pragma unroll 1
                 for (int blk = 0; blk < W / NP; ++blk) {
@@ -418,83 +430,93 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
         __syncthreads();
 
         // ------------------------------------------------------------ phase B
-        // map g: P[i][k] at maps[g*MS + i*N + k], z[i] at maps[g*MS + N*N + i]
+        // maps (aliasing the window buffers): zero, then column k of chunk g's
+        // P from lane k, z from the zero-state lane; identity beyond Gb.
+        for (int e = tid; e < Gp * MS; e += THREADS) maps[e] = T(0);
+        __syncthreads();
         if (active) {
             T *Mg = maps + (size_t)grp * MS;
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
                 if (i < N) {
                     if (!xlane)
-                        Mg[i * N + kk] = h[NP - 1 - i];
+                        Mg[i * RS + kk] = h[NP - 1 - i];
                     else
-                        Mg[N * N + i] = h[NP - 1 - i];
+                        Mg[NP * RS + i] = h[NP - 1 - i];
                 }
             }
         }
-        // identity maps pad the tree to a power of two
-        for (int e = tid; e < (Gp - Gb) * MS; e += THREADS) {
-            const int g = Gb + e / MS;
-            const int r = e - (g - Gb) * MS;
-            T v = T(0);
-            if (r < N * N && (r / N) == (r % N)) v = T(1);
-            maps[(size_t)g * MS + r] = v;
+        for (int e = tid; e < (Gp - Gb) * N; e += THREADS) {
+            const int g = Gb + e / N;
+            const int i = e - (g - Gb) * N;
+            maps[(size_t)g * MS + i * RS + i] = T(1);
         }
         __syncthreads();
-        // up-sweep: M[j] <- M[j] o M[i]  (i = j - d; apply M[i] first)
+        // up-sweep: M[j] <- M[j] o M[i] (i = j - d: M[i] acts first).  One
+        // thread per output row keeps the row in registers.
         for (int d = 1; d < Gp; d <<= 1) {
             const int npairs = Gp / (2 * d);
-            const int tot = npairs * MS;
-            for (int e = tid; e < tot; e += THREADS) {
-                const int m = e / MS;
-                const int r = e - m * MS;
-                const int j = 2 * d * m + 2 * d - 1;
-                const int i = j - d;
-                const T *Pj = maps + (size_t)j * MS;
-                const T *Mi = maps + (size_t)i * MS;
-                T acc;
-                if (r < N * N) {
-                    const int row = r / N, col = r - row * N;
-                    acc = T(0);
-                    for (int q = 0; q < N; ++q) acc = fma(Pj[row * N + q], Mi[q * N + col], acc);
-                } else {
-                    const int row = r - N * N;
-                    acc = Pj[N * N + row];
-                    for (int q = 0; q < N; ++q) acc = fma(Pj[row * N + q], Mi[N * N + q], acc);
+            const int pslots = THREADS / NP;
+            for (int base = 0; base < npairs; base += pslots) {
+                const int m = base + tid / NP;
+                const int row = tid % NP;
+                const bool on = (tid / NP) < pslots && m < npairs;
+                T acc[NP];
+                T accz = T(0);
+                if (on) {
+                    const int j = 2 * d * m + 2 * d - 1;
+                    const int i = j - d;
+                    const T *Pj = maps + (size_t)j * MS + row * RS;
+                    const T *Mi = maps + (size_t)i * MS;
+#pragma unroll
+                    for (int c = 0; c < NP; ++c) acc[c] = T(0);
+                    accz = maps[(size_t)j * MS + NP * RS + row];
+#pragma unroll
+                    for (int q = 0; q < NP; ++q) {
+                        const T pq = Pj[q];
+                        T mrow[NP];
+                        lds_row<T, NP>(mrow, Mi + q * RS);
+#pragma unroll
+                        for (int c = 0; c < NP; ++c) acc[c] = fma(pq, mrow[c], acc[c]);
+                        accz = fma(pq, Mi[NP * RS + q], accz);
+                    }
                 }
-                tmpm[e] = acc;
+                __syncthreads();
+                if (on) {
+                    const int j = 2 * d * m + 2 * d - 1;
+                    T *Pj = maps + (size_t)j * MS + row * RS;
+#pragma unroll
+                    for (int c = 0; c < NP; ++c) Pj[c] = acc[c];
+                    maps[(size_t)j * MS + NP * RS + row] = accz;
+                }
+                __syncthreads();
             }
-            __syncthreads();
-            for (int e = tid; e < tot; e += THREADS) {
-                const int m = e / MS;
-                const int r = e - m * MS;
-                const int j = 2 * d * m + 2 * d - 1;
-                maps[(size_t)j * MS + r] = tmpm[e];
-            }
-            __syncthreads();
         }
 
         // ------------------------------------------------------------ phase C
         // publish the aggregate (root), look back, publish the inclusive state
         const int64_t me = ticket;
         const T *root = maps + (size_t)(Gp - 1) * MS;
-        double *s_in = sin_d;
         if (kb == 0) {
-            if (tid < N) {
+            if (tid < NP) {
                 double v = 0.0;
-                if (!REV && p.zi) v = (double)p.zi[b * N + tid];
+                if (!REV && p.zi && tid < N) v = (double)p.zi[b * N + tid];
                 s_in[tid] = v;
             }
         } else {
-            for (int e = tid; e < N * N; e += THREADS) p.aggP[(size_t)me * N * N + e] = root[e];
-            for (int e = tid; e < N; e += THREADS) p.aggz[(size_t)me * N + e] = (double)root[N * N + e];
+            for (int e = tid; e < N * N; e += THREADS) {
+                const int r = e / N, c = e - (e / N) * N;
+                p.aggP[(size_t)me * N * N + e] = root[r * RS + c];
+            }
+            for (int e = tid; e < N; e += THREADS) p.aggz[(size_t)me * N + e] = (double)root[NP * RS + e];
             __threadfence();
             __syncthreads();
             if (tid == 0) st_release(p.flags + me, kFlagAgg);
             if (tid < 32) {
                 // warp 0: walk back to the nearest inclusive state
-                int64_t m = kb - 1;
                 int64_t found = -1;
                 if (tid == 0) {
+                    int64_t m = kb - 1;
                     for (;;) {
                         if (m < 0) {  // cannot happen: batch 0 always publishes an inclusive state
                             atomicOr(p.status, 2u);
@@ -520,18 +542,22 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
                             found = m;
                             break;
                         }
-                        --m;  // aggregate only; batch 0 always publishes an inclusive state
+                        --m;  // aggregate only: keep walking
                     }
                     misc[1] = found;
                 }
                 __syncwarp();
                 found = misc[1];
-                        if (found == -2) {
-                    if (tid < N) s_in[tid] = 0.0;
+                if (found == -2) {
+                    if (tid < NP) s_in[tid] = 0.0;
                 } else {
-                    if (tid < N) {
-                        (void)ld_acquire(p.flags + found * p.B + b);
-                        s_in[tid] = p.incl[(size_t)(found * p.B + b) * N + tid];
+                    if (tid < NP) {
+                        double v = 0.0;
+                        if (tid < N) {
+                            (void)ld_acquire(p.flags + found * p.B + b);
+                            v = p.incl[(size_t)(found * p.B + b) * N + tid];
+                        }
+                        s_in[tid] = v;
                     }
                     __syncwarp();
                     // compose aggregates found+1 .. kb-1 (all published: we walked past them)
@@ -555,97 +581,71 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
         // inclusive state of this batch: root applied to s_in
         if (kb + 1 < p.nbps) {
             if (tid < N) {
-                double v = (double)root[N * N + tid];
-                for (int q = 0; q < N; ++q) v = fma((double)root[tid * N + q], s_in[q], v);
+                double v = (double)root[NP * RS + tid];
+                for (int q = 0; q < N; ++q) v = fma((double)root[tid * RS + q], s_in[q], v);
                 p.incl[(size_t)me * N + tid] = v;
             }
             __threadfence();
             __syncthreads();
             if (tid == 0) st_release(p.flags + me, kFlagInc);
         }
-
-        // down-sweep: exclusive prefixes (root <- identity)
-        for (int e = tid; e < MS; e += THREADS) {
-            T v = T(0);
-            if (e < N * N && (e / N) == (e % N)) v = T(1);
-            maps[(size_t)(Gp - 1) * MS + e] = v;
-        }
+        // down-sweep on states (FP64): left child <- parent's entry state,
+        // right child <- left subtree's aggregate applied to it.
+        for (int e = tid; e < Gp * NP; e += THREADS) st[e] = 0.0;
+        __syncthreads();
+        if (tid < NP) st[(size_t)(Gp - 1) * NP + tid] = s_in[tid];
         __syncthreads();
         for (int d = Gp / 2; d >= 1; d >>= 1) {
             const int npairs = Gp / (2 * d);
-            const int tot = npairs * MS;
-            // left child <- parent prefix; right child <- left-subtree total o parent prefix
-            for (int e = tid; e < tot; e += THREADS) {
-                const int m = e / MS;
-                const int r = e - m * MS;
+            for (int base = 0; base < npairs * NP; base += THREADS) {
+                const int e = base + tid;
+                const bool on = e < npairs * NP;
+                const int m = e / NP;
+                const int row = e - m * NP;
                 const int j = 2 * d * m + 2 * d - 1;
                 const int i = j - d;
-                const T *Ti = maps + (size_t)i * MS;  // left-subtree total
-                const T *Pp = maps + (size_t)j * MS;  // parent prefix
-                T acc;
-                if (r < N * N) {
-                    const int row = r / N, col = r - row * N;
-                    acc = T(0);
-                    for (int q = 0; q < N; ++q) acc = fma(Ti[row * N + q], Pp[q * N + col], acc);
-                } else {
-                    const int row = r - N * N;
-                    acc = Ti[N * N + row];
-                    for (int q = 0; q < N; ++q) acc = fma(Ti[row * N + q], Pp[N * N + q], acc);
+                double v = 0.0;
+                if (on) {
+                    const T *Mi = maps + (size_t)i * MS;
+                    const double *par = st + (size_t)j * NP;
+                    v = (double)Mi[NP * RS + row];
+#pragma unroll
+                    for (int q = 0; q < NP; ++q) v = fma((double)Mi[row * RS + q], par[q], v);
                 }
-                tmpm[e] = acc;
+                __syncthreads();
+                if (on) {
+                    st[(size_t)i * NP + row] = st[(size_t)j * NP + row];
+                    st[(size_t)j * NP + row] = v;
+                }
+                __syncthreads();
             }
-            __syncthreads();
-            for (int e = tid; e < tot; e += THREADS) {
-                const int m = e / MS;
-                const int r = e - m * MS;
-                const int j = 2 * d * m + 2 * d - 1;
-                const int i = j - d;
-                maps[(size_t)i * MS + r] = maps[(size_t)j * MS + r];
-                maps[(size_t)j * MS + r] = tmpm[e];
-            }
-            __syncthreads();
         }
-        // entry state of chunk g: E_g(s_in)
-        for (int e = tid; e < Gb * N; e += THREADS) {
-            const int g = e / N;
-            const int i = e - g * N;
-            const T *Eg = maps + (size_t)g * MS;
-            double v = (double)Eg[N * N + i];
-            for (int q = 0; q < N; ++q) v = fma((double)Eg[i * N + q], s_in[q], v);
-            ent[e] = (T)v;
-        }
-        __syncthreads();
 
         // ------------------------------------------------------------ phase D
+        // fix-up: one lane per chunk re-runs the chunk from its entry state
         if (N < NP)
-            for (int e = tid; e < 2 * G * W * NP; e += THREADS)
-                if (e % NP >= N) Abuf[e] = T(0);
+            for (int e = tid; e < 2 * G * GS; e += THREADS)
+                if ((e % GS) % NP >= N) Abuf[e] = T(0);
         const bool fix = tid < Gb;
 #pragma unroll
-        for (int j = 0; j < NP; ++j) h[j] = T(0);
-        if (fix) {
-#pragma unroll
-            for (int i = 0; i < NP; ++i)
-                if (i < N) h[NP - 1 - i] = ent[tid * N + i];
-        }
-        // time-invariant grad_A: per-thread partial sums of one tap
+        for (int i = 0; i < NP; ++i) h[NP - 1 - i] = (fix && i < N) ? (T)st[(size_t)tid * NP + i] : T(0);
         const bool ti = REV && p.gA && p.as_t == 0;
         __syncthreads();
         Loader<T, NP, REV>::load(p, vec, b, tb, Gb, 0, Abuf, ibuf, ybuf, REV);
         cp_async_commit();
         for (int w = 0; w < nwin; ++w) {
-            T *As = Abuf + (size_t)(w & 1) * G * W * NP;
-            T *xs = ibuf + (size_t)(w & 1) * G * W;
-            T *ys = ybuf + (size_t)(w & 1) * G * (W + NP);
+            const T *As = Abuf + (size_t)(w & 1) * G * GS;
+            const T *xs = ibuf + (size_t)(w & 1) * G * W;
+            const T *ys = ybuf + (size_t)(w & 1) * G * (W + NP);
             if (w + 1 < nwin)
-                Loader<T, NP, REV>::load(p, vec, b, tb, Gb, w + 1, Abuf + (size_t)((w + 1) & 1) * G * W * NP,
+                Loader<T, NP, REV>::load(p, vec, b, tb, Gb, w + 1, Abuf + (size_t)((w + 1) & 1) * G * GS,
                                          ibuf + (size_t)((w + 1) & 1) * G * W,
                                          ybuf + (size_t)((w + 1) & 1) * G * (W + NP), REV);
             cp_async_commit();
             cp_async_wait<1>();
             __syncthreads();
             if (fix) {
-                const T *Ag = As + (size_t)tid * W * NP;
+                const T *Ag = As + (size_t)tid * GS;
                 const T *xg = xs + (size_t)tid * W;
                 T *og = obuf + (size_t)tid * W;
 #pragma unroll 1
@@ -667,8 +667,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
             }
             __syncthreads();
             // flush the window's outputs
-            const int tot = Gb * W;
-            for (int e = tid; e < tot; e += THREADS) {
+            for (int e = tid; e < Gb * W; e += THREADS) {
                 const int g = e / W;
                 const int j = e - g * W;
                 const int64_t pos = tb + (int64_t)g * p.L + (int64_t)w * W + j;  // step index
@@ -679,36 +678,53 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
             }
             if (REV && p.gA) {
                 const T sgn = NEG ? T(1) : T(-1);
-                if (!ti) {
-                    // rows t in [top-W, top-1] are contiguous: flat (row, tap) order
-                    const int per = W * N;
-                    const int totg = Gb * per;
-                    for (int e = tid; e < totg; e += THREADS) {
-                        const int g = e / per;
-                        const int remg = e - g * per;
-                        const int rr = remg / N;  // row offset from the lowest time in the window
-                        const int i = remg - rr * N;
-                        const int s = W - 1 - rr;  // slot of that time
+                if (!ti && vec && NP % V == 0) {
+                    // rows t in [top-W, top-1] are contiguous: one 16-byte vector of
+                    // taps per thread and step
+                    constexpr int QR = NP / V;     // vectors per row
+                    constexpr int QPC = W * QR;    // vectors per chunk window
+                    using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+                    for (int e = tid; e < Gb * QPC; e += THREADS) {
+                        const int g = e / QPC;
+                        const int remg = e - g * QPC;
+                        const int rr = remg / QR;  // row offset from the lowest time in the window
+                        const int i0 = (remg - rr * QR) * V;
+                        const int s = W - 1 - rr;
                         const int64_t pos = tb + (int64_t)g * p.L + (int64_t)w * W + s;
                         if (pos >= p.T) continue;
                         const int64_t t = p.T - 1 - pos;
-                        const T gx = obuf[g * W + s];
-                        const T yv = ys[g * (W + NP) + s + i];
-                        p.gA[(b * p.T + t) * N + i] = sgn * gx * yv;
+                        const T gx = sgn * obuf[g * W + s];
+                        const T *yq = ys + g * (W + NP) + s + i0;
+                        VT o;
+                        T *ov = reinterpret_cast<T *>(&o);
+#pragma unroll
+                        for (int j = 0; j < V; ++j) ov[j] = gx * yq[j];
+                        *reinterpret_cast<VT *>(p.gA + (b * p.T + t) * NP + i0) = o;
                     }
-                } else {
-                    const int totg = Gb * W * N;
-                    for (int e = tid; e < totg; e += THREADS) {
-                        // tap fixed per thread across windows: e % N is stable when THREADS % N == 0;
-                        // otherwise accumulate per element into the same register (still one tap per e)
-                        const int g = e / (W * N);
-                        const int remg = e - g * (W * N);
-                        const int s = remg / N;
-                        const int i = remg - s * N;
+                } else if (!ti) {
+                    const int per = W * N;
+                    for (int e = tid; e < Gb * per; e += THREADS) {
+                        const int g = e / per;
+                        const int remg = e - g * per;
+                        const int rr = remg / N;
+                        const int i = remg - rr * N;
+                        const int s = W - 1 - rr;
                         const int64_t pos = tb + (int64_t)g * p.L + (int64_t)w * W + s;
                         if (pos >= p.T) continue;
-                        const T v = sgn * obuf[g * W + s] * ys[g * (W + NP) + s + i];
-                        atomicAdd(p.gA + b * N + i, v);
+                        const int64_t t = p.T - 1 - pos;
+                        p.gA[(b * p.T + t) * N + i] = sgn * obuf[g * W + s] * ys[g * (W + NP) + s + i];
+                    }
+                } else {
+                    // time-invariant coefficients: per-thread partial sums per tap, added atomically
+                    for (int i = tid % NP; i < N; i += NP) {
+                        T acc = T(0);
+                        for (int e = tid / NP; e < Gb * W; e += THREADS / NP) {
+                            const int g = e / W;
+                            const int sl = e - g * W;
+                            const int64_t pos = tb + (int64_t)g * p.L + (int64_t)w * W + sl;
+                            if (pos < p.T) acc = fma(obuf[e], ys[g * (W + NP) + sl + i], acc);
+                        }
+                        if (acc != T(0)) atomicAdd(p.gA + b * N + i, sgn * acc);
                     }
                 }
             }
