@@ -42,6 +42,7 @@ namespace {
 constexpr unsigned kFlagAgg = 1u;
 constexpr unsigned kFlagInc = 2u;
 constexpr int kHeaderBytes = 256;  // ticket counter, status word, padding
+constexpr int kLookbackRing = 4;    // predecessor aggregates prefetched ahead of the composition
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
@@ -98,7 +99,7 @@ struct ChunkParams {
 
 template <int NP>
 struct Cfg {
-    static constexpr int THREADS = NP <= 16 ? 512 : 256;
+    static constexpr int THREADS = 256;
     static constexpr int W = NP * ((16 + NP - 1) / NP);  // steps per window, multiple of NP
 };
 
@@ -155,7 +156,7 @@ __device__ __forceinline__ void lds_row(T (&dst)[NP], const T *src) {
 
 // Shared-memory plan (bytes), all regions 16-byte aligned.
 struct SmemPlan {
-    size_t abuf, ibuf, obuf, ybuf, maps, st, sin, misc, total;
+    size_t abuf, ibuf, obuf, ybuf, maps, st, sin, lbP, lbz, misc, total;
     __host__ __device__ SmemPlan(size_t esz, int NP, int W, int G, int N, bool rev) {
         auto al = [](size_t v) { return (v + 15) & ~size_t(15); };
         size_t off = 0;
@@ -178,6 +179,10 @@ struct SmemPlan {
         off += al((size_t)Gp * NP * sizeof(double));
         sin = off;
         off += al((size_t)NP * sizeof(double));
+        lbP = off;  // look-back ring: predecessor aggregates in flight
+        off += al((size_t)kLookbackRing * NP * NP * esz);
+        lbz = off;
+        off += al((size_t)kLookbackRing * NP * sizeof(double));
         misc = off;
         off += 64;
         total = off;
@@ -343,7 +348,7 @@ struct Loader {
 // The kernel.
 // ----------------------------------------------------------------------------
 template <typename T, int NP, bool REV, bool NEG>
-__global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chunked_kernel(ChunkParams<T> p) {
+__global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParams<T> p) {
     constexpr int W = Cfg<NP>::W;
     constexpr int THREADS = Cfg<NP>::THREADS;
     constexpr int V = 16 / sizeof(T);
@@ -513,18 +518,18 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
             __syncthreads();
             if (tid == 0) st_release(p.flags + me, kFlagAgg);
             if (tid < 32) {
-                // warp 0: walk back to the nearest inclusive state
+                // warp 0: parallel look-back.  Lane l watches predecessor
+                // kb-1-l-32r; a round ends when every watched batch has
+                // published; the nearest inclusive state ends the walk.
+                const int lane = tid;
                 int64_t found = -1;
-                if (tid == 0) {
-                    int64_t m = kb - 1;
-                    for (;;) {
-                        if (m < 0) {  // cannot happen: batch 0 always publishes an inclusive state
-                            atomicOr(p.status, 2u);
-                            found = -2;
-                            break;
-                        }
-                        const int64_t idx = m * p.B + b;
-                        unsigned f = ld_acquire(p.flags + idx);
+                bool timeout = false;
+                for (int64_t hi = kb - 1; hi >= 0 && found < 0 && !timeout; hi -= 32) {
+                    const int64_t m = hi - lane;
+                    unsigned f = kFlagInc;  // batches before 0 do not exist: treat as resolved
+                    if (m >= 0) {
+                        const unsigned *fp = p.flags + m * p.B + b;
+                        f = ld_acquire(fp);
                         unsigned n = 0;
                         while (f == 0u) {
                             if (++n > p.spin_limit || ld_acquire(p.status) != 0u) {
@@ -532,48 +537,70 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
                                 break;
                             }
                             __nanosleep(32);
-                            f = ld_acquire(p.flags + idx);
+                            f = ld_acquire(fp);
                         }
-                        if (f == 0u) {  // timed out: give up with a zero state
-                            found = -2;
-                            break;
-                        }
-                        if (f == kFlagInc) {
-                            found = m;
-                            break;
-                        }
-                        --m;  // aggregate only: keep walking
                     }
-                    misc[1] = found;
+                    timeout = __any_sync(0xffffffffu, f == 0u);
+                    const unsigned inc = __ballot_sync(0xffffffffu, f == kFlagInc && m >= 0);
+                    if (inc) found = hi - (__ffs(inc) - 1);
                 }
-                __syncwarp();
-                found = misc[1];
-                if (found == -2) {
+                if (found < 0 && !timeout) {  // cannot happen: batch 0 always publishes an inclusive state
+                    if (lane == 0) atomicOr(p.status, 2u);
+                    timeout = true;
+                }
+                // the flags seen above were acquired lane by lane; order every
+                // lane's reads of the predecessors' data after them
+                __threadfence();
+                if (timeout) {
                     if (tid < NP) s_in[tid] = 0.0;
                 } else {
                     if (tid < NP) {
                         double v = 0.0;
-                        if (tid < N) {
-                            (void)ld_acquire(p.flags + found * p.B + b);
-                            v = p.incl[(size_t)(found * p.B + b) * N + tid];
-                        }
+                        if (tid < N) v = p.incl[(size_t)(found * p.B + b) * N + tid];
                         s_in[tid] = v;
                     }
                     __syncwarp();
-                    // compose aggregates found+1 .. kb-1 (all published: we walked past them)
-                    for (int64_t mm = found + 1; mm < kb; ++mm) {
-                        const int64_t idx = mm * p.B + b;
+                    // compose the aggregates found+1 .. kb-1 in order; their data is
+                    // pulled into a shared-memory ring kLookbackRing hops ahead
+                    T *lbP = reinterpret_cast<T *>(smem + S.lbP);
+                    double *lbz = reinterpret_cast<double *>(smem + S.lbz);
+                    const int64_t m0 = found + 1;
+                    const int64_t K = kb - m0;
+                    auto fetch = [&](int64_t hop) {
+                        if (hop < K) {
+                            const int64_t idx = (m0 + hop) * p.B + b;
+                            T *dP = lbP + (size_t)(hop % kLookbackRing) * NP * NP;
+                            double *dz = lbz + (size_t)(hop % kLookbackRing) * NP;
+                            for (int e = lane; e < N * N; e += 32) {
+                                const int r = e / N, c = e - (e / N) * N;
+                                cp_async<sizeof(T)>(dP + r * NP + c, p.aggP + (size_t)idx * N * N + e);
+                            }
+                            if (lane < N) cp_async<8>(dz + lane, p.aggz + (size_t)idx * N + lane);
+                        }
+                        cp_async_commit();
+                    };
+#pragma unroll
+                    for (int hop = 0; hop < kLookbackRing; ++hop) fetch(hop);
+                    for (int64_t hop = 0; hop < K; ++hop) {
+                        cp_async_wait<kLookbackRing - 1>();
+                        __syncwarp();
                         double v = 0.0;
-                        if (tid < N) {
-                            (void)ld_acquire(p.flags + idx);
-                            const T *Pm = p.aggP + (size_t)idx * N * N + (size_t)tid * N;
-                            v = p.aggz[(size_t)idx * N + tid];
-                            for (int q = 0; q < N; ++q) v = fma((double)Pm[q], s_in[q], v);
+                        if (lane < N) {
+                            const T *Pr = lbP + (size_t)(hop % kLookbackRing) * NP * NP + lane * NP;
+                            double v0 = lbz[(hop % kLookbackRing) * NP + lane], v1 = 0.0;
+#pragma unroll
+                            for (int q = 0; q < NP; q += 2) {
+                                if (q < N) v0 = fma((double)Pr[q], s_in[q], v0);
+                                if (q + 1 < N) v1 = fma((double)Pr[q + 1], s_in[q + 1], v1);
+                            }
+                            v = v0 + v1;
                         }
                         __syncwarp();
-                        if (tid < N) s_in[tid] = v;
+                        if (lane < N) s_in[lane] = v;
                         __syncwarp();
+                        fetch(hop + kLookbackRing);
                     }
+                    cp_async_wait<0>();
                 }
             }
         }
@@ -757,7 +784,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 1024 / Cfg<NP>::THREADS) chu
 constexpr int kChunkLen = 128;   // target chunk length; rounded to a multiple of the window
 constexpr int kMaxChunksPerBatch = 64;
 
-inline int threads_for(int NP) { return NP <= 16 ? 512 : 256; }
+inline int threads_for(int) { return 256; }
 inline int window_for(int NP) { return NP * ((16 + NP - 1) / NP); }
 
 struct Plan {
