@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the per-config summary")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--B", type=int, default=None, help="override signals (scaled-down instance for profiling)")
+    ap.add_argument("--T", type=int, default=None, help="override samples per signal (scaled-down instance)")
     return ap.parse_args()
 
 
@@ -137,10 +139,10 @@ def bytes_per_sample(N: int, time_invariant: bool):
 
 
 # --------------------------------------------------------------------------- workloads
-def load_workload(cfg: str, device, seed: int = 0):
+def load_workload(cfg: str, device, seed: int = 0, B=None, T=None):
     from torchlpc_b200.synth import make_workload
 
-    return make_workload(cfg, seed=seed, device=device)
+    return make_workload(cfg, seed=seed, device=device, B=B, T=T)
 
 
 def samples_of(w) -> int:
@@ -395,7 +397,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
     device = "cuda" if torch.cuda.is_available() else "cpu"
-    w = load_workload(args.config, device)
+    w = load_workload(args.config, device, B=args.B, T=args.T)
     once, nsamp, desc = reference_calls(ref, w)
     for _ in range(max(1, args.warmup)):
         once()
@@ -434,7 +436,7 @@ def run_ours(args):
 
     assert tl.EXTENSION_LOADED
     tl.set_algo(args.algo)
-    w = load_workload(args.config, device, seed=rk)
+    w = load_workload(args.config, device, seed=rk, B=args.B, T=args.T)
     if w["workload"].ragged:
         w["offsets_dev"] = w["offsets"].to(device)
     wl = w["workload"]
