@@ -89,6 +89,27 @@ int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A,
                       size_t workspace_bytes, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Forward filter with no workspace argument, for callers that cannot allocate
+ * device memory (code that must not call an allocator, such as a real-time
+ * audio thread or a host callback, or an FFI binding without a memory
+ * manager).  No counterpart in the reference: torchlpc always allocates
+ * through torch.
+ * Runs the chunked kernel with scratch taken from an 8 MiB array compiled
+ * into this library (held on every GPU that loads it, until exit).  Returns
+ * LPC_ERR_WORKSPACE when the problem needs more scratch than that (roughly
+ * 12 million samples per call at order 16), LPC_ERR_UNSUPPORTED for orders
+ * above 32.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call shares the one array: calls whose work overlaps on the GPU
+ * (different streams, or several host threads) race and must be serialised
+ * by the caller.  Nothing is allocated or freed.
+ * ------------------------------------------------------------------------- */
+int lpc_b200_forward_noalloc(int dtype, const void *x, const void *A,
+                             const void *zi, void *y, int64_t B, int64_t T,
+                             int64_t N, int64_t a_stride_b, int64_t a_stride_t,
+                             void *stream);
+
+/* ---------------------------------------------------------------------------
  * Order-1 recurrence  out[t] = decay[t]*out[t-1] + impulse[t],  out[-1]=init.
  * Replaces the reference operator torchlpc::scan(impulse, decay, init)
  *   (torchlpc/csrc/scan_cpu.cpp:28-78,124-141; linear_recurrence.cu:232-291;

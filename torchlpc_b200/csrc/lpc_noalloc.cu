@@ -1,0 +1,82 @@
+// Forward filter for callers that cannot allocate device memory.
+//
+// The chunked forward kernel needs scratch memory in global memory (a ticket
+// counter, a status word, one flag, aggregate and inclusive state per batch of
+// chunks).  lpc_b200_forward takes that scratch as a caller-supplied
+// workspace.  Some callers cannot provide one: code that runs where no
+// allocator may be called (inside a host callback, from a real-time audio
+// thread that must not block on the driver's allocator, from a plugin host
+// that owns all device memory), or code that has no allocator at all (a thin
+// FFI binding with no memory manager).  This entry point serves them with a
+// fixed scratch array that lives in the library itself.
+//
+// The array is a file-scope __device__ variable, so every GPU that loads this
+// library holds kStaticScratchBytes of device memory until the process exits.
+// Its host-side name is only a stand-in for the symbol: the device address is
+// looked up with cudaGetSymbolAddress once per device, on the first call made
+// while that device is current, and cached.
+#include <mutex>
+
+#include "lpc_chunked.cuh"
+
+using namespace lpcb;
+
+namespace {
+
+// 8 MiB: enough for about 6,500 batches of chunks, i.e. roughly 12 million
+// samples per call at order 16 (the scratch grows with the number of batches
+// and with N^2).
+constexpr size_t kStaticScratchBytes = size_t(8) << 20;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+std::mutex g_setup_mutex;
+void *g_scratch_addr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device (looked up once).
+int scratch_for_current_device(void **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return LPC_ERR_CUDA;
+    if (dev < 0 || dev >= kMaxDevices) return LPC_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (g_scratch_addr[dev] == nullptr) {
+        void *ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || ptr == nullptr) return LPC_ERR_CUDA;
+        g_scratch_addr[dev] = ptr;
+    }
+    *out = g_scratch_addr[dev];
+    return LPC_OK;
+}
+
+template <typename T>
+int run(const void *x, const void *A, const void *zi, void *y, int64_t B, int64_t T_, int64_t N, int64_t sb,
+        int64_t st, void *scratch, cudaStream_t stream) {
+    FwdArgs<T> p{static_cast<const T *>(x), static_cast<const T *>(A), static_cast<const T *>(zi),
+                 static_cast<T *>(y), B, T_, N, sb, st};
+    // chunked_forward clears the counter, status word and flags of the scratch
+    // on `stream` before the kernel runs; the rest is written before it is read
+    return chunked_forward<T>(p, false, scratch, kStaticScratchBytes, stream) == cudaSuccess ? LPC_OK
+                                                                                              : LPC_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int lpc_b200_forward_noalloc(int dtype, const void *x, const void *A, const void *zi, void *y,
+                                        int64_t B, int64_t T, int64_t N, int64_t a_stride_b,
+                                        int64_t a_stride_t, void *stream) {
+    if (dtype != LPC_F32 && dtype != LPC_F64) return LPC_ERR_INVALID_ARGUMENT;
+    if (B < 0 || T < 0 || N < 1 || N > kMaxOrder || B >= (int64_t(1) << 31)) return LPC_ERR_INVALID_ARGUMENT;
+    if (B > 0 && T > 0 && (!x || !A || !y)) return LPC_ERR_INVALID_ARGUMENT;
+    if (a_stride_t < 0 || a_stride_b < 0 || (a_stride_t != 0 && a_stride_t < N)) return LPC_ERR_INVALID_ARGUMENT;
+    if (!chunked_supported(N)) return LPC_ERR_UNSUPPORTED;  // orders above 32 have no chunked kernel
+    if (B == 0 || T == 0) return LPC_OK;
+    const size_t esz = dtype == LPC_F32 ? 4 : 8;
+    if (chunked_forward_workspace(esz, B, T, N, a_stride_t) > kStaticScratchBytes) return LPC_ERR_WORKSPACE;
+    void *scratch = nullptr;
+    const int rc = scratch_for_current_device(&scratch);
+    if (rc != LPC_OK) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == LPC_F32) return run<float>(x, A, zi, y, B, T, N, a_stride_b, a_stride_t, scratch, s);
+    return run<double>(x, A, zi, y, B, T, N, a_stride_b, a_stride_t, scratch, s);
+}
