@@ -25,11 +25,14 @@
 //     (the coefficient windows are streamed again; they are L2-resident by
 //     then) and the CTA writes the outputs back coalesced.
 //
-// The backward runs the same machinery over reversed time on grad_y with the
-// diagonal coefficients A[t+1+i, i] (skewed into shared memory so a step's
-// taps are contiguous) and fuses grad_A = -grad_x[t] * y[t-1-i] into the
-// phase-D epilogue (time-invariant A: a per-CTA reduction added atomically);
-// the CTA that owns t = 0 derives grad_zi from grad_x[0..N-1].
+// The backward runs the same machinery over reversed time on grad_y: the
+// adjoint recurrence grad_x[t] = grad_y[t] - sum_i A[t+1+i,i] grad_x[t+1+i] in
+// transposed (scatter) form, where producing grad_x[t] adds -A[t,i]*grad_x[t]
+// to the pending accumulator of output t-1-i.  Its state is the N pending
+// accumulators and each step reads one contiguous row A[t,:], so both
+// directions stream the same row windows.  grad_A = -grad_x[t] * y[t-1-i] is
+// fused into the phase-D epilogue (time-invariant A: per-tap sums added
+// atomically); grad_zi is the adjoint carried N steps past t = 0.
 #include "lpc_chunked.cuh"
 
 namespace lpcb {
@@ -42,7 +45,7 @@ namespace {
 constexpr unsigned kFlagAgg = 1u;
 constexpr unsigned kFlagInc = 2u;
 constexpr int kHeaderBytes = 256;  // ticket counter, status word, padding
-constexpr int kLookbackRing = 4;    // predecessor aggregates prefetched ahead of the composition
+constexpr int kLookbackChunk = 8;   // predecessor aggregates staged per round of the composition
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
@@ -136,6 +139,26 @@ __device__ __forceinline__ T step_dot(const T (&a)[NP], const T (&h)[NP], int u,
     }
 }
 
+// Transposed (scatter) form for the adjoint recurrence: c[(u+i) mod NP] is the
+// pending accumulator of the output i steps ahead; the step's output consumes
+// c[u] and scatters -a[i]*out into the rest, so a step reads one contiguous
+// coefficient row.
+template <typename T, int NP>
+__device__ __forceinline__ T step_scatter(const T (&a)[NP], T (&c)[NP], int u, T in) {
+    const T g = in + c[u];
+    c[u] = T(0);
+#pragma unroll
+    for (int i = 0; i < NP; ++i) c[(u + 1 + i) % NP] = fma(-a[i], g, c[(u + 1 + i) % NP]);
+    return g;
+}
+
+// Ring position of logical state element i at a window boundary (u = 0):
+// direct form s[i] = y[t0-1-i] at h[NP-1-i]; transposed form c[i] at c[i].
+template <bool REV, int NP>
+__device__ __forceinline__ constexpr int state_slot(int i) {
+    return REV ? i : NP - 1 - i;
+}
+
 template <typename T, int NP>
 __device__ __forceinline__ void lds_row(T (&dst)[NP], const T *src) {
     if constexpr (sizeof(T) * NP % 16 == 0) {
@@ -179,10 +202,10 @@ struct SmemPlan {
         off += al((size_t)Gp * NP * sizeof(double));
         sin = off;
         off += al((size_t)NP * sizeof(double));
-        lbP = off;  // look-back ring: predecessor aggregates in flight
-        off += al((size_t)kLookbackRing * NP * NP * esz);
+        lbP = off;  // look-back stages: predecessor aggregates (two stages of kLookbackChunk)
+        off += al((size_t)2 * kLookbackChunk * NP * NP * esz);
         lbz = off;
-        off += al((size_t)kLookbackRing * NP * sizeof(double));
+        off += al((size_t)2 * kLookbackChunk * NP * sizeof(double));
         misc = off;
         off += 64;
         total = off;
@@ -192,8 +215,10 @@ struct SmemPlan {
 
 // ----------------------------------------------------------------------------
 // Window loaders.  Window w of chunk g covers steps [w*W, w*W+W) of the chunk.
-// Forward: step j of chunk g is time t = tb + g*L + j (tb: batch start).
-// Backward: step j is reversed time tau = tb + g*L + j, i.e. t = T-1-tau.
+// Forward: step j is time t = tb + g*L + w*W + j, stored at slot j.
+// Backward: step j is time t = top-1-j (top = T - (tb + g*L + w*W)), stored at
+// slot t - (top - W) = W-1-j.  Either way a window is a run of W consecutive
+// coefficient rows in natural order; rows outside [0, T) read as zero.
 // ----------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ bool is_aligned16(const void *p) {
@@ -207,11 +232,27 @@ struct Loader {
     static constexpr int V = 16 / sizeof(T);
     static constexpr int GS = group_stride(W, NP, sizeof(T));
 
-    // Vector fast path: order equals the padded order, rows are dense and
-    // 16-byte aligned, so every index below divides by a compile-time constant.
+    // Vector fast path: order equals the padded order, rows are dense, 16-byte
+    // multiples and 16-byte aligned, so every index below divides by a
+    // compile-time constant.
     __device__ static bool fast(const ChunkParams<T> &p) {
         return p.N == NP && p.as_t == NP && NP % V == 0 && (p.as_b * (int64_t)sizeof(T)) % 16 == 0 &&
                is_aligned16<T>(p.A);
+    }
+
+    // First row held by slot 0 of chunk g's window w, and the valid slot range.
+    __device__ static void rows(const ChunkParams<T> &p, int64_t tb, int g, int w, int64_t &row0, int &lo,
+                                int &hi) {
+        if (!REV) {
+            row0 = tb + (int64_t)g * p.L + (int64_t)w * W;
+            lo = 0;
+            hi = (int)max64(0, min64(W, p.T - row0));
+        } else {
+            const int64_t top = p.T - (tb + (int64_t)g * p.L + (int64_t)w * W);
+            row0 = top - W;
+            lo = (int)min64(W, max64(0, -row0));
+            hi = W;
+        }
     }
 
     __device__ static void load(const ChunkParams<T> &p, bool vec, int64_t b, int64_t tb, int Gb, int w,
@@ -220,125 +261,71 @@ struct Loader {
         const int tid = threadIdx.x;
         const T *Ab = p.A + b * p.as_b;
         const T *inb = p.in + b * p.T;
-        if (!REV) {
-            if (vec) {
-                constexpr int VPW = W * NP / V;  // vectors per chunk window
-                for (int e = tid; e < Gb * VPW; e += THREADS) {
-                    const int g = e / VPW;
-                    const int v = e - g * VPW;
-                    const int64_t t0 = tb + (int64_t)g * p.L + (int64_t)w * W;
-                    T *dst = As + (size_t)g * GS + v * V;
-                    const T *src = Ab + t0 * NP + v * V;
-                    if (t0 + W <= p.T) {
-                        cp_async<16>(dst, src);
-                    } else {
+        if (vec) {
+            constexpr int RV = NP / V;       // vectors per row
+            constexpr int VPW = W * RV;      // vectors per chunk window
+            for (int e = tid; e < Gb * VPW; e += THREADS) {
+                const int g = e / VPW;
+                const int v = e - g * VPW;
+                const int r = v / RV;
+                int64_t row0;
+                int lo, hi;
+                rows(p, tb, g, w, row0, lo, hi);
+                T *dst = As + (size_t)g * GS + v * V;
+                if (r >= lo && r < hi) {
+                    cp_async<16>(dst, Ab + row0 * NP + v * V);
+                } else {
 #pragma unroll
-                        for (int j = 0; j < V; ++j) {
-                            const int64_t t = t0 + (v * V + j) / NP;
-                            if (t < p.T)
-                                cp_async<sizeof(T)>(dst + j, src + j);
-                            else
-                                dst[j] = T(0);
-                        }
-                    }
+                    for (int j = 0; j < V; ++j) dst[j] = T(0);
                 }
-            } else {
-                const int per = W * N;
-                for (int e = tid; e < Gb * per; e += THREADS) {
-                    const int g = e / per;
-                    const int rem = e - g * per;
-                    const int r = rem / N;
-                    const int i = rem - r * N;
-                    const int64_t t = tb + (int64_t)g * p.L + (int64_t)w * W + r;
-                    T *dst = As + (size_t)g * GS + r * NP + i;
-                    if (t < p.T)
-                        cp_async<sizeof(T)>(dst, Ab + t * p.as_t + i);
-                    else
-                        *dst = T(0);
-                }
-            }
-            for (int e = tid; e < Gb * W; e += THREADS) {
-                const int g = e / W;
-                const int r = e - g * W;
-                const int64_t t = tb + (int64_t)g * p.L + (int64_t)w * W + r;
-                if (t < p.T)
-                    cp_async<sizeof(T)>(xs + e, inb + t);
-                else
-                    xs[e] = T(0);
             }
         } else {
-            // skewed diagonal: slot (s, i) <- A[top - s + i, i] (zero outside [0, T)),
-            // top = T - (first reversed step of the window)
-            if (vec) {
-                constexpr int RV = NP / V;              // vectors per row
-                constexpr int VPC = (W + NP - 1) * RV;  // vectors per chunk window
-                for (int e = tid; e < Gb * VPC; e += THREADS) {
-                    const int g = e / VPC;
-                    const int rem = e - g * VPC;
-                    const int q = rem / RV;
-                    const int i0 = (rem - q * RV) * V;
-                    const int64_t top = p.T - (tb + (int64_t)g * p.L + (int64_t)w * W);
-                    const int64_t r = top - (W - 1) + q;
-                    T *Ag = As + (size_t)g * GS;
-                    const bool in_range = (r >= 0 && r < p.T);
-                    const T *src = Ab + r * NP + i0;
-#pragma unroll
-                    for (int j = 0; j < V; ++j) {
-                        const int i = i0 + j;
-                        const int s = (int)(top - r) + i;
-                        if (s < 0 || s >= W) continue;
-                        if (in_range)
-                            cp_async<sizeof(T)>(Ag + s * NP + i, src + j);
-                        else
-                            Ag[s * NP + i] = T(0);
-                    }
-                }
-            } else {
-                const int span = W + N - 1;
-                const int per = span * N;
-                for (int e = tid; e < Gb * per; e += THREADS) {
-                    const int g = e / per;
-                    const int rem = e - g * per;
-                    const int q = rem / N;
-                    const int i = rem - q * N;
-                    const int64_t top = p.T - (tb + (int64_t)g * p.L + (int64_t)w * W);
-                    const int64_t r = top - (W - 1) + q;
-                    const int s = (int)(top - r) + i;
-                    if (s < 0 || s >= W) continue;
-                    T *dst = As + (size_t)g * GS + s * NP + i;
-                    if (r >= 0 && r < p.T)
-                        cp_async<sizeof(T)>(dst, Ab + r * p.as_t + i);
-                    else
-                        *dst = T(0);
-                }
-            }
-            for (int e = tid; e < Gb * W; e += THREADS) {
-                const int g = e / W;
-                const int s = e - g * W;
-                const int64_t t = p.T - 1 - (tb + (int64_t)g * p.L + (int64_t)w * W + s);
-                if (t >= 0)
-                    cp_async<sizeof(T)>(xs + e, inb + t);
+            const int per = W * N;
+            for (int e = tid; e < Gb * per; e += THREADS) {
+                const int g = e / per;
+                const int rem = e - g * per;
+                const int r = rem / N;
+                const int i = rem - r * N;
+                int64_t row0;
+                int lo, hi;
+                rows(p, tb, g, w, row0, lo, hi);
+                T *dst = As + (size_t)g * GS + r * NP + i;
+                if (r >= lo && r < hi)
+                    cp_async<sizeof(T)>(dst, Ab + (row0 + r) * p.as_t + i);
                 else
-                    xs[e] = T(0);
+                    *dst = T(0);
             }
-            if (with_y) {
-                // ys[g][q] = ypad(top - 2 - q), q in [0, W + NP)
-                const T *yb = p.ysave + b * p.T;
-                const T *zib = p.zi ? p.zi + b * N : nullptr;
-                constexpr int PY = W + NP;
-                for (int e = tid; e < Gb * PY; e += THREADS) {
-                    const int g = e / PY;
-                    const int q = e - g * PY;
-                    const int64_t top = p.T - (tb + (int64_t)g * p.L + (int64_t)w * W);
-                    const int64_t j = top - 2 - q;
-                    T *dst = ys + e;
-                    if (j >= 0 && j < p.T)
-                        cp_async<sizeof(T)>(dst, yb + j);
-                    else if (j < 0 && -1 - j < N && zib)
-                        *dst = zib[-1 - j];
-                    else
-                        *dst = T(0);
-                }
+        }
+        // inputs (x forward, grad_y backward), slot r <-> index row0 + r
+        for (int e = tid; e < Gb * W; e += THREADS) {
+            const int g = e / W;
+            const int r = e - g * W;
+            int64_t row0;
+            int lo, hi;
+            rows(p, tb, g, w, row0, lo, hi);
+            if (r >= lo && r < hi)
+                cp_async<sizeof(T)>(xs + e, inb + row0 + r);
+            else
+                xs[e] = T(0);
+        }
+        if (REV && with_y) {
+            // ys[g][q] = ypad(top - 2 - q), q in [0, W + NP): the lagged outputs
+            // y[t-1-i] of the window's steps (y[-1-k] = zi[k])
+            const T *yb = p.ysave + b * p.T;
+            const T *zib = p.zi ? p.zi + b * N : nullptr;
+            constexpr int PY = W + NP;
+            for (int e = tid; e < Gb * PY; e += THREADS) {
+                const int g = e / PY;
+                const int q = e - g * PY;
+                const int64_t top = p.T - (tb + (int64_t)g * p.L + (int64_t)w * W);
+                const int64_t j = top - 2 - q;
+                T *dst = ys + e;
+                if (j >= 0 && j < p.T)
+                    cp_async<sizeof(T)>(dst, yb + j);
+                else if (j < 0 && -1 - j < N && zib)
+                    *dst = zib[-1 - j];
+                else
+                    *dst = T(0);
             }
         }
     }
@@ -348,7 +335,7 @@ struct Loader {
 // The kernel.
 // ----------------------------------------------------------------------------
 template <typename T, int NP, bool REV, bool NEG>
-__global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParams<T> p) {
+__global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_kernel(ChunkParams<T> p) {
     constexpr int W = Cfg<NP>::W;
     constexpr int THREADS = Cfg<NP>::THREADS;
     constexpr int V = 16 / sizeof(T);
@@ -397,7 +384,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParam
         const bool xlane = (kk == N);
         T h[NP];
 #pragma unroll
-        for (int j = 0; j < NP; ++j) h[j] = (active && !xlane && j == NP - 1 - kk) ? T(1) : T(0);
+        for (int j = 0; j < NP; ++j) h[j] = (active && !xlane && j == state_slot<REV, NP>(kk)) ? T(1) : T(0);
 
         Loader<T, NP, REV>::load(p, vec, b, tb, Gb, 0, Abuf, ibuf, nullptr, false);
         cp_async_commit();
@@ -418,14 +405,18 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParam
 #pragma unroll
                     for (int u = 0; u < NP; ++u) {
                         const int j = blk * NP + u;
+                        const int slot = REV ? W - 1 - j : j;
                         T a[NP];
-                        lds_row<T, NP>(a, Ag + (size_t)j * NP);
+                        lds_row<T, NP>(a, Ag + (size_t)slot * NP);
                         if constexpr (NEG) {
 #pragma unroll
                             for (int i = 0; i < NP; ++i) a[i] = -a[i];
                         }
-                        const T in = xlane ? xg[j] : T(0);
-                        h[u] = step_dot<T, NP>(a, h, u, in);
+                        const T in = xlane ? xg[slot] : T(0);
+                        if constexpr (REV)
+                            step_scatter<T, NP>(a, h, u, in);
+                        else
+                            h[u] = step_dot<T, NP>(a, h, u, in);
                     }
                 }
             }
@@ -444,10 +435,11 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParam
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
                 if (i < N) {
+                    const T v = h[state_slot<REV, NP>(i)];
                     if (!xlane)
-                        Mg[i * RS + kk] = h[NP - 1 - i];
+                        Mg[i * RS + kk] = v;
                     else
-                        Mg[NP * RS + i] = h[NP - 1 - i];
+                        Mg[NP * RS + i] = v;
                 }
             }
         }
@@ -553,55 +545,75 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParam
                 __threadfence();
                 if (timeout) {
                     if (tid < NP) s_in[tid] = 0.0;
-                } else {
-                    if (tid < NP) {
-                        double v = 0.0;
-                        if (tid < N) v = p.incl[(size_t)(found * p.B + b) * N + tid];
-                        s_in[tid] = v;
-                    }
-                    __syncwarp();
-                    // compose the aggregates found+1 .. kb-1 in order; their data is
-                    // pulled into a shared-memory ring kLookbackRing hops ahead
-                    T *lbP = reinterpret_cast<T *>(smem + S.lbP);
-                    double *lbz = reinterpret_cast<double *>(smem + S.lbz);
-                    const int64_t m0 = found + 1;
-                    const int64_t K = kb - m0;
-                    auto fetch = [&](int64_t hop) {
-                        if (hop < K) {
-                            const int64_t idx = (m0 + hop) * p.B + b;
-                            T *dP = lbP + (size_t)(hop % kLookbackRing) * NP * NP;
-                            double *dz = lbz + (size_t)(hop % kLookbackRing) * NP;
-                            for (int e = lane; e < N * N; e += 32) {
-                                const int r = e / N, c = e - (e / N) * N;
-                                cp_async<sizeof(T)>(dP + r * NP + c, p.aggP + (size_t)idx * N * N + e);
-                            }
-                            if (lane < N) cp_async<8>(dz + lane, p.aggz + (size_t)idx * N + lane);
-                        }
-                        cp_async_commit();
-                    };
-#pragma unroll
-                    for (int hop = 0; hop < kLookbackRing; ++hop) fetch(hop);
-                    for (int64_t hop = 0; hop < K; ++hop) {
-                        cp_async_wait<kLookbackRing - 1>();
-                        __syncwarp();
-                        double v = 0.0;
-                        if (lane < N) {
-                            const T *Pr = lbP + (size_t)(hop % kLookbackRing) * NP * NP + lane * NP;
-                            double v0 = lbz[(hop % kLookbackRing) * NP + lane], v1 = 0.0;
-#pragma unroll
-                            for (int q = 0; q < NP; q += 2) {
-                                if (q < N) v0 = fma((double)Pr[q], s_in[q], v0);
-                                if (q + 1 < N) v1 = fma((double)Pr[q + 1], s_in[q + 1], v1);
-                            }
-                            v = v0 + v1;
-                        }
-                        __syncwarp();
-                        if (lane < N) s_in[lane] = v;
-                        __syncwarp();
-                        fetch(hop + kLookbackRing);
-                    }
-                    cp_async_wait<0>();
+                } else if (tid < NP) {
+                    double v = 0.0;
+                    if (tid < N) v = p.incl[(size_t)(found * p.B + b) * N + tid];
+                    s_in[tid] = v;
                 }
+                if (tid == 0) misc[1] = timeout ? -1 : found;
+            }
+            __syncthreads();
+            // compose the aggregates found+1 .. kb-1 in order.  The whole CTA
+            // streams them into a double-buffered shared stage, kLookbackChunk
+            // hops at a time, while warp 0 applies the previous stage.
+            const int64_t found = misc[1];
+            if (found >= 0) {
+                T *lbP = reinterpret_cast<T *>(smem + S.lbP);
+                double *lbz = reinterpret_cast<double *>(smem + S.lbz);
+                const int64_t m0 = found + 1;
+                const int64_t K = kb - m0;
+                const int64_t nch = (K + kLookbackChunk - 1) / kLookbackChunk;
+                const int per = N * N + N;
+                auto issue = [&](int64_t c) {
+                    const int64_t h0 = c * kLookbackChunk;
+                    const int nh = (int)min64(kLookbackChunk, K - h0);
+                    T *dP = lbP + (size_t)(c & 1) * kLookbackChunk * NP * NP;
+                    double *dz = lbz + (size_t)(c & 1) * kLookbackChunk * NP;
+                    for (int e = tid; e < nh * per; e += THREADS) {
+                        const int hh = e / per;
+                        const int r = e - hh * per;
+                        const int64_t idx = (m0 + h0 + hh) * p.B + b;
+                        if (r < N * N) {
+                            const int row = r / N, col = r - (r / N) * N;
+                            cp_async<sizeof(T)>(dP + (size_t)hh * NP * NP + row * NP + col,
+                                                p.aggP + (size_t)idx * N * N + r);
+                        } else {
+                            cp_async<8>(dz + (size_t)hh * NP + (r - N * N), p.aggz + (size_t)idx * N + (r - N * N));
+                        }
+                    }
+                };
+                if (nch > 0) issue(0);
+                cp_async_commit();
+                for (int64_t c = 0; c < nch; ++c) {
+                    if (c + 1 < nch) issue(c + 1);
+                    cp_async_commit();
+                    cp_async_wait<1>();
+                    __syncthreads();
+                    if (tid < 32) {
+                        const int lane = tid;
+                        const int nh = (int)min64(kLookbackChunk, K - c * kLookbackChunk);
+                        const T *P0 = lbP + (size_t)(c & 1) * kLookbackChunk * NP * NP;
+                        const double *z0 = lbz + (size_t)(c & 1) * kLookbackChunk * NP;
+                        for (int hh = 0; hh < nh; ++hh) {
+                            double v = 0.0;
+                            if (lane < N) {
+                                const T *Pr = P0 + (size_t)hh * NP * NP + lane * NP;
+                                double v0 = z0[hh * NP + lane], v1 = 0.0;
+#pragma unroll
+                                for (int q = 0; q < NP; q += 2) {
+                                    if (q < N) v0 = fma((double)Pr[q], s_in[q], v0);
+                                    if (q + 1 < N) v1 = fma((double)Pr[q + 1], s_in[q + 1], v1);
+                                }
+                                v = v0 + v1;
+                            }
+                            __syncwarp();
+                            if (lane < N) s_in[lane] = v;
+                            __syncwarp();
+                        }
+                    }
+                    __syncthreads();
+                }
+                cp_async_wait<0>();
             }
         }
         __syncthreads();
@@ -655,7 +667,8 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParam
                 if ((e % GS) % NP >= N) Abuf[e] = T(0);
         const bool fix = tid < Gb;
 #pragma unroll
-        for (int i = 0; i < NP; ++i) h[NP - 1 - i] = (fix && i < N) ? (T)st[(size_t)tid * NP + i] : T(0);
+        for (int i = 0; i < NP; ++i)
+            h[state_slot<REV, NP>(i)] = (fix && i < N) ? (T)st[(size_t)tid * NP + i] : T(0);
         const bool ti = REV && p.gA && p.as_t == 0;
         __syncthreads();
         Loader<T, NP, REV>::load(p, vec, b, tb, Gb, 0, Abuf, ibuf, ybuf, REV);
@@ -677,19 +690,26 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParam
                 T *og = obuf + (size_t)tid * W;
 #pragma unroll 1
                 for (int blk = 0; blk < W / NP; ++blk) {
+                    T o[NP];
 #pragma unroll
                     for (int u = 0; u < NP; ++u) {
                         const int j = blk * NP + u;
+                        const int slot = REV ? W - 1 - j : j;
                         T a[NP];
-                        lds_row<T, NP>(a, Ag + (size_t)j * NP);
+                        lds_row<T, NP>(a, Ag + (size_t)slot * NP);
                         if constexpr (NEG) {
 #pragma unroll
                             for (int i = 0; i < NP; ++i) a[i] = -a[i];
                         }
-                        h[u] = step_dot<T, NP>(a, h, u, xg[j]);
+                        if constexpr (REV) {
+                            o[u] = step_scatter<T, NP>(a, h, u, xg[slot]);
+                        } else {
+                            h[u] = step_dot<T, NP>(a, h, u, xg[slot]);
+                            o[u] = h[u];
+                        }
                     }
 #pragma unroll
-                    for (int u = 0; u < NP; ++u) og[blk * NP + u] = h[u];
+                    for (int u = 0; u < NP; ++u) og[blk * NP + u] = o[u];
                 }
             }
             __syncthreads();
@@ -701,6 +721,9 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParam
                 if (pos < p.T) {
                     const int64_t t = REV ? p.T - 1 - pos : pos;
                     p.out[b * p.T + t] = obuf[e];
+                } else if (REV && p.gzi && pos - p.T < N) {
+                    // steps past t = 0 carry the adjoint into the initial conditions
+                    p.gzi[b * N + (pos - p.T)] = obuf[e];
                 }
             }
             if (REV && p.gA) {
@@ -758,21 +781,14 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, 4) chunked_kernel(ChunkParam
             __syncthreads();
         }
         cp_async_wait<0>();
-        // grad_zi from grad_x[0..N-1]: owned by the batch that contains t = 0
-        if (REV && p.gzi && tb + (int64_t)Gb * p.L >= p.T) {
-            __syncthreads();
-            if (tid < N) {
-                const int k = tid;
-                const T *Ab = p.A + b * p.as_b;
-                T acc = T(0);
-                // grad_x[j] for j < T - tb was written by this CTA; beyond that
-                // it is the batch's entry state (owned by the previous batch)
-                const int64_t own = p.T - tb;
-                for (int j = 0; j + k < N && j < p.T; ++j) {
-                    const T gxj = j < own ? p.out[b * p.T + j] : (T)s_in[j - own];
-                    acc = fma(Ab[j * p.as_t + j + k], gxj, acc);
-                }
-                p.gzi[b * N + k] = NEG ? acc : -acc;
+        // grad_zi entries beyond the padded steps of the signal's last chunk are
+        // still pending in that chunk's exit state
+        if (REV && p.gzi && kb + 1 == p.nbps && tid == Gb - 1) {
+            const int64_t npad = tb + (int64_t)Gb * p.L - p.T;  // steps of the chunk with t < 0
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                const int64_t k = npad + i;
+                if (i < N && k < N) p.gzi[b * N + k] = h[state_slot<REV, NP>(i)];
             }
         }
     }
