@@ -12,18 +12,22 @@
 //  A  "lanes = filters": every chunk gets N+1 lanes, N basis filters and one
 //     zero-state filter, each holding its N-tap history in registers.  The
 //     coefficient rows of the chunk are staged per window of W steps into
-//     shared memory with cp.async (double buffered) and read as broadcasts
-//     (one 16-byte shared load feeds every lane of the chunk).
+//     shared memory with cp.async (double buffered, 16-byte vectors when the
+//     rows allow) and read as broadcasts (one 16-byte shared load feeds every
+//     lane of the chunk).  Half-way through, the lanes also store the map of
+//     the chunk's first half.
 //  B  a Blelloch tree over the G affine maps in shared memory: the batch
 //     aggregate (up-sweep) and each chunk's exclusive prefix (down-sweep).
 //  C  decoupled look-back over the predecessor batches of the same signal:
-//     the aggregate is published, predecessors' aggregates are composed in
-//     FP64 until an inclusive state is found, the batch's inclusive state is
-//     published (FP64).  Every spin-wait is bounded; on expiry the kernel
-//     records LPC_ERR_TIMEOUT in the workspace status word and moves on.
-//  D  fix-up: one lane per chunk re-runs its chunk from the exact entry state
-//     (the coefficient windows are streamed again; they are L2-resident by
-//     then) and the CTA writes the outputs back coalesced.
+//     the aggregate is published, predecessors' aggregates are staged into
+//     shared memory and composed in FP64 until an inclusive state is found,
+//     the batch's inclusive state is published (FP64).  Every wait is
+//     bounded; on expiry the kernel records a bit in the workspace status
+//     word and moves on.
+//  D  fix-up: one lane per half-chunk re-runs it from its exact entry state
+//     (second halves start from the first half's map applied to the chunk's
+//     entry state, in FP64); the coefficient windows are streamed again (they
+//     are L2-resident by then) and the CTA writes the outputs back coalesced.
 //
 // The backward runs the same machinery over reversed time on grad_y: the
 // adjoint recurrence grad_x[t] = grad_y[t] - sum_i A[t+1+i,i] grad_x[t+1+i] in
@@ -31,8 +35,9 @@
 // to the pending accumulator of output t-1-i.  Its state is the N pending
 // accumulators and each step reads one contiguous row A[t,:], so both
 // directions stream the same row windows.  grad_A = -grad_x[t] * y[t-1-i] is
-// fused into the phase-D epilogue (time-invariant A: per-tap sums added
-// atomically); grad_zi is the adjoint carried N steps past t = 0.
+// fused into the phase-D epilogue (time-invariant A: a separate reduction
+// kernel over the grad_x just written); grad_zi is the adjoint carried N steps
+// past t = 0.
 #include "lpc_chunked.cuh"
 
 namespace lpcb {
@@ -45,23 +50,46 @@ namespace {
 constexpr unsigned kFlagAgg = 1u;
 constexpr unsigned kFlagInc = 2u;
 constexpr int kHeaderBytes = 256;  // ticket counter, status word, padding
-constexpr int kLookbackChunk = 8;   // predecessor aggregates staged per round of the composition
+// Predecessor aggregates staged per round of the look-back composition
+// (about 4 KB of coefficients per round).
+__host__ __device__ constexpr int lookback_hops(int NP, int esz) {
+    return 4096 / (NP * NP * esz) < 2 ? 2 : (4096 / (NP * NP * esz) > 8 ? 8 : 4096 / (NP * NP * esz));
+}
+
+// Window loaders: per-element cp.async (any layout) or 16-byte cp.async per
+// vector (dense rows of the padded order, 16-byte rows and windows, 16-byte
+// aligned signal starts).
+constexpr int kLoadElem = 0;
+constexpr int kLoadVec = 1;
+
+// Status bits a bounded wait records before giving up.
+constexpr unsigned kStatusFlagWait = 1u;     // a predecessor's flag never appeared
+constexpr unsigned kStatusNoInclusive = 2u;  // look-back ran past batch 0 (cannot happen)
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// A published aggregate is stored padded to the padded order: P as NP rows of
+// NP (zeros beyond N), z as NP doubles, each record a multiple of 16 bytes so
+// that it can be moved with 16-byte vector loads.
+__host__ __device__ constexpr int agg_p_elems(int NP, int esz) {
+    return ((NP * NP * esz + 15) / 16) * 16 / esz;
+}
+__host__ __device__ constexpr int agg_z_elems(int NP) { return ((NP * 8 + 15) / 16) * 2; }
 
 struct WsLayout {
     size_t flags, aggP, aggz, incl, total;
 };
 
 inline WsLayout ws_layout(size_t esz, int64_t nbatches, int64_t N) {
+    const int NP = padded_order(N);
     WsLayout l;
     size_t off = kHeaderBytes;
     l.flags = off;
     off = align256(off + (size_t)nbatches * 4);
     l.aggP = off;
-    off = align256(off + (size_t)nbatches * N * N * esz);
+    off = align256(off + (size_t)nbatches * agg_p_elems(NP, (int)esz) * esz);
     l.aggz = off;
-    off = align256(off + (size_t)nbatches * N * 8);
+    off = align256(off + (size_t)nbatches * agg_z_elems(NP) * 8);
     l.incl = off;
     off = align256(off + (size_t)nbatches * N * 8);
     l.total = off;
@@ -91,11 +119,12 @@ struct ChunkParams {
     int N;
     int L;           // chunk length (multiple of the window)
     int G;           // chunks per batch
+    int loader;      // window loader: kLoadElem or kLoadVec
     int64_t nbps;    // batches per signal
     int64_t nbatches;
     unsigned *counter, *status, *flags;
-    F *aggP;         // [nbatches][N][N]
-    double *aggz;    // [nbatches][N]
+    F *aggP;         // [nbatches][agg_p_elems]
+    double *aggz;    // [nbatches][agg_z_elems]
     double *incl;    // [nbatches][N]
     unsigned spin_limit;
 };
@@ -103,19 +132,24 @@ struct ChunkParams {
 template <int NP>
 struct Cfg {
     static constexpr int THREADS = 256;
-    static constexpr int W = NP * ((16 + NP - 1) / NP);  // steps per window, multiple of NP
+    static constexpr int W = NP * ((16 + NP - 1) / NP);  // phase-A window: steps, a multiple of NP
+    static constexpr int WD = W / 2;                     // phase-D window (half-chunks, half the steps)
 };
 
-// Per-chunk stride of a coefficient window in shared memory: W rows of NP plus
-// one 16-byte pad so that the rows different chunks read in the same step
-// fall in different banks.
-__host__ __device__ constexpr int group_stride(int W, int NP, int esz) { return W * NP + 16 / esz; }
+// Per-chunk stride of a coefficient window in shared memory: WC rows of NP
+// plus one 16-byte pad so that the rows different chunks read in the same
+// step fall in different banks.
+__host__ __device__ constexpr int group_stride(int WC, int NP, int esz) { return WC * NP + 16 / esz; }
 // Row stride of a stored affine map (16-byte aligned, padded against bank conflicts).
 __host__ __device__ constexpr int map_row_stride(int NP, int esz) {
     return ((NP + 16 / esz - 1) / (16 / esz)) * (16 / esz) + 16 / esz;
 }
 __host__ __device__ constexpr int map_stride(int NP, int esz) {
     return NP * map_row_stride(NP, esz) + ((NP + 16 / esz - 1) / (16 / esz)) * (16 / esz);
+}
+// Half-chunk map (P rows of NP, then z), padded to 16 bytes.
+__host__ __device__ constexpr int half_map_elems(int NP, int esz) {
+    return ((NP * NP + NP) * esz + 15) / 16 * 16 / esz;
 }
 
 // acc - sum_i a[i] * h[(u-1-i) mod NP] with two partial chains (even/odd taps)
@@ -177,159 +211,254 @@ __device__ __forceinline__ void lds_row(T (&dst)[NP], const T *src) {
     }
 }
 
-// Shared-memory plan (bytes), all regions 16-byte aligned.
+// Shared-memory plan (bytes), all regions 16-byte aligned.  The window
+// buffers of phases A and D alias the tree maps and the look-back stage:
+// phases B and C run between the two window loops.
 struct SmemPlan {
-    size_t abuf, ibuf, obuf, ybuf, maps, st, sin, lbP, lbz, misc, total;
-    __host__ __device__ SmemPlan(size_t esz, int NP, int W, int G, int N, bool rev) {
+    size_t abuf, ibuf, obuf, ybuf, maps, half, st, sin, lbP, lbz, misc, total;
+    __host__ __device__ SmemPlan(size_t esz, int NP, int G, bool rev) {
         auto al = [](size_t v) { return (v + 15) & ~size_t(15); };
+        const int W = NP * ((16 + NP - 1) / NP), WD = W / 2;
         size_t off = 0;
         abuf = off;
-        const size_t abytes = al((size_t)2 * G * group_stride(W, NP, (int)esz) * esz);
-        // the tree maps alias the window buffers (phases B/C run between the
-        // window loops of phases A and D)
+        const size_t awin = al((size_t)2 * G * group_stride(W, NP, (int)esz) * esz);
+        const size_t dwin = al((size_t)2 * 2 * G * group_stride(WD, NP, (int)esz) * esz);
         int Gp = 1;
         while (Gp < G) Gp <<= 1;
         const size_t mapbytes = al((size_t)Gp * map_stride(NP, (int)esz) * esz);
+        const int KL = lookback_hops(NP, (int)esz);
+        const size_t lbPbytes = al((size_t)2 * KL * agg_p_elems(NP, (int)esz) * esz);
+        const size_t lbzbytes = al((size_t)2 * KL * agg_z_elems(NP) * sizeof(double));
         maps = off;
-        off += al(abytes > mapbytes ? abytes : mapbytes);
-        ibuf = off;
+        lbP = off + mapbytes;
+        lbz = lbP + lbPbytes;
+        size_t r = mapbytes + lbPbytes + lbzbytes;
+        if (awin > r) r = awin;
+        if (dwin > r) r = dwin;
+        off += al(r);
+        ibuf = off;  // inputs: 2 stages x G x W (= 2 stages x 2G x WD)
         off += al((size_t)2 * G * W * esz);
-        obuf = off;
-        off += al((size_t)G * W * esz);
-        ybuf = off;
-        if (rev) off += al((size_t)2 * G * (W + NP) * esz);
+        obuf = off;  // phase-D outputs of one window
+        off += al((size_t)2 * G * WD * esz);
+        ybuf = off;  // backward: lagged outputs y of the phase-D windows
+        if (rev) off += al((size_t)2 * 2 * G * (WD + NP) * esz);
+        half = off;  // map over the first half of each chunk
+        off += al((size_t)G * half_map_elems(NP, (int)esz) * esz);
         st = off;  // FP64 entry states of the tree nodes
         off += al((size_t)Gp * NP * sizeof(double));
         sin = off;
         off += al((size_t)NP * sizeof(double));
-        lbP = off;  // look-back stages: predecessor aggregates (two stages of kLookbackChunk)
-        off += al((size_t)2 * kLookbackChunk * NP * NP * esz);
-        lbz = off;
-        off += al((size_t)2 * kLookbackChunk * NP * sizeof(double));
-        misc = off;
+        misc = off;  // ticket
         off += 64;
         total = off;
-        (void)N;
     }
 };
 
 // ----------------------------------------------------------------------------
-// Window loaders.  Window w of chunk g covers steps [w*W, w*W+W) of the chunk.
-// Forward: step j is time t = tb + g*L + w*W + j, stored at slot j.
-// Backward: step j is time t = top-1-j (top = T - (tb + g*L + w*W)), stored at
-// slot t - (top - W) = W-1-j.  Either way a window is a run of W consecutive
-// coefficient rows in natural order; rows outside [0, T) read as zero.
+// Window loaders.  Window w (WC steps) of chunk g (Lc steps) covers steps
+// [w*WC, w*WC+WC) of the chunk.
+// Forward: step j is time t = tb + g*Lc + w*WC + j, stored at slot j.
+// Backward: step j is time t = top-1-j (top = T - (tb + g*Lc + w*WC)),
+// stored at slot t - (top - WC) = WC-1-j.  Either way a window is a run of WC
+// consecutive coefficient rows in natural order; rows outside [0, T) read as
+// zero.  Backward windows also carry the lagged outputs
+// ys[g][r] = ypad(top-WC-NP+r), r in [0, WC+NP), natural order, with
+// ypad(-1-k) = zi[k] (zero past k = N-1).
 // ----------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ bool is_aligned16(const void *p) {
     return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
 }
 
-template <typename T, int NP, bool REV>
+template <typename T, int NP, bool REV, int WC>
 struct Loader {
-    static constexpr int W = Cfg<NP>::W;
     static constexpr int THREADS = Cfg<NP>::THREADS;
-    static constexpr int V = 16 / sizeof(T);
-    static constexpr int GS = group_stride(W, NP, sizeof(T));
-
-    // Vector fast path: order equals the padded order, rows are dense, 16-byte
-    // multiples and 16-byte aligned, so every index below divides by a
-    // compile-time constant.
-    __device__ static bool fast(const ChunkParams<T> &p) {
-        return p.N == NP && p.as_t == NP && NP % V == 0 && (p.as_b * (int64_t)sizeof(T)) % 16 == 0 &&
-               is_aligned16<T>(p.A);
-    }
+    static constexpr int GS = group_stride(WC, NP, sizeof(T));
+    static constexpr int PY = WC + NP;
 
     // First row held by slot 0 of chunk g's window w, and the valid slot range.
-    __device__ static void rows(const ChunkParams<T> &p, int64_t tb, int g, int w, int64_t &row0, int &lo,
-                                int &hi) {
+    __device__ static void rows(const ChunkParams<T> &p, int64_t tb, int Lc, int g, int w, int64_t &row0,
+                                int &lo, int &hi) {
         if (!REV) {
-            row0 = tb + (int64_t)g * p.L + (int64_t)w * W;
+            row0 = tb + (int64_t)g * Lc + (int64_t)w * WC;
             lo = 0;
-            hi = (int)max64(0, min64(W, p.T - row0));
+            hi = (int)max64(0, min64(WC, p.T - row0));
         } else {
-            const int64_t top = p.T - (tb + (int64_t)g * p.L + (int64_t)w * W);
-            row0 = top - W;
-            lo = (int)min64(W, max64(0, -row0));
-            hi = W;
+            const int64_t top = p.T - (tb + (int64_t)g * Lc + (int64_t)w * WC);
+            row0 = top - WC;
+            lo = (int)min64(WC, max64(0, -row0));
+            hi = WC;
         }
     }
 
-    __device__ static void load(const ChunkParams<T> &p, bool vec, int64_t b, int64_t tb, int Gb, int w,
-                                T *As, T *xs, T *ys, bool with_y) {
-        const int N = p.N;
+    // Vector path: all threads, one 16-byte cp.async per vector of a chunk's
+    // rows, inputs and lagged outputs.  The caller commits the group.
+    __device__ static void load_vec(const ChunkParams<T> &p, int64_t b, int64_t tb, int Gc, int Lc, int w,
+                                    T *As, T *xs, T *ys, bool with_y) {
+        constexpr int V = 16 / sizeof(T);
+        constexpr int RV = NP / V > 0 ? NP / V : 1;  // vectors per row
+        constexpr int AV = WC * RV;                  // coefficient vectors per chunk window
+        constexpr int XV = WC / V > 0 ? WC / V : 1;  // input vectors
+        constexpr int YV = PY / V;                   // lagged-output vectors
+        const int per = AV + XV + ((REV && with_y) ? YV : 0);
         const int tid = threadIdx.x;
         const T *Ab = p.A + b * p.as_b;
         const T *inb = p.in + b * p.T;
-        if (vec) {
-            constexpr int RV = NP / V;       // vectors per row
-            constexpr int VPW = W * RV;      // vectors per chunk window
-            for (int e = tid; e < Gb * VPW; e += THREADS) {
-                const int g = e / VPW;
-                const int v = e - g * VPW;
-                const int r = v / RV;
-                int64_t row0;
-                int lo, hi;
-                rows(p, tb, g, w, row0, lo, hi);
-                T *dst = As + (size_t)g * GS + v * V;
+        for (int e = tid; e < Gc * per; e += THREADS) {
+            const int g = e / per;
+            const int q = e - g * per;
+            int64_t row0;
+            int lo, hi;
+            rows(p, tb, Lc, g, w, row0, lo, hi);
+            if (q < AV) {
+                const int r = q / RV;
+                T *dst = As + (size_t)g * GS + q * V;
                 if (r >= lo && r < hi) {
-                    cp_async<16>(dst, Ab + row0 * NP + v * V);
+                    cp_async<16>(dst, Ab + row0 * NP + q * V);
                 } else {
 #pragma unroll
                     for (int j = 0; j < V; ++j) dst[j] = T(0);
                 }
-            }
-        } else {
-            const int per = W * N;
-            for (int e = tid; e < Gb * per; e += THREADS) {
-                const int g = e / per;
-                const int rem = e - g * per;
-                const int r = rem / N;
-                const int i = rem - r * N;
-                int64_t row0;
-                int lo, hi;
-                rows(p, tb, g, w, row0, lo, hi);
-                T *dst = As + (size_t)g * GS + r * NP + i;
-                if (r >= lo && r < hi)
-                    cp_async<sizeof(T)>(dst, Ab + (row0 + r) * p.as_t + i);
-                else
-                    *dst = T(0);
+            } else if (q < AV + XV) {
+                const int r = (q - AV) * V;  // lo, hi and r are multiples of V
+                T *dst = xs + (size_t)g * WC + r;
+                if (r >= lo && r < hi) {
+                    cp_async<16>(dst, inb + row0 + r);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < V; ++j) dst[j] = T(0);
+                }
+            } else {
+                const int r = (q - AV - XV) * V;
+                T *dst = ys + (size_t)g * PY + r;
+                const int64_t j0 = row0 - NP + r;  // a multiple of V: all or none of the vector is before t = 0
+                if (j0 >= 0) {
+                    cp_async<16>(dst, p.ysave + b * p.T + j0);
+                } else {
+                    const T *zib = p.zi ? p.zi + b * p.N : nullptr;
+#pragma unroll
+                    for (int j = 0; j < V; ++j) {
+                        const int64_t k = -1 - (j0 + j);
+                        dst[j] = (k >= 0 && k < p.N && zib) ? zib[k] : T(0);
+                    }
+                }
             }
         }
-        // inputs (x forward, grad_y backward), slot r <-> index row0 + r
-        for (int e = tid; e < Gb * W; e += THREADS) {
-            const int g = e / W;
-            const int r = e - g * W;
+    }
+
+    // Element path: all threads, one cp.async per element (any stride and
+    // alignment).  The caller commits the group.
+    __device__ static void load_elem(const ChunkParams<T> &p, int64_t b, int64_t tb, int Gc, int Lc, int w,
+                                     T *As, T *xs, T *ys, bool with_y) {
+        const int N = p.N;
+        const int tid = threadIdx.x;
+        const T *Ab = p.A + b * p.as_b;
+        const T *inb = p.in + b * p.T;
+        const int per = WC * N;
+        for (int e = tid; e < Gc * per; e += THREADS) {
+            const int g = e / per;
+            const int rem = e - g * per;
+            const int r = rem / N;
+            const int i = rem - r * N;
             int64_t row0;
             int lo, hi;
-            rows(p, tb, g, w, row0, lo, hi);
+            rows(p, tb, Lc, g, w, row0, lo, hi);
+            T *dst = As + (size_t)g * GS + r * NP + i;
+            if (r >= lo && r < hi)
+                cp_async<sizeof(T)>(dst, Ab + (row0 + r) * p.as_t + i);
+            else
+                *dst = T(0);
+        }
+        // inputs (x forward, grad_y backward), slot r <-> index row0 + r
+        for (int e = tid; e < Gc * WC; e += THREADS) {
+            const int g = e / WC;
+            const int r = e - g * WC;
+            int64_t row0;
+            int lo, hi;
+            rows(p, tb, Lc, g, w, row0, lo, hi);
             if (r >= lo && r < hi)
                 cp_async<sizeof(T)>(xs + e, inb + row0 + r);
             else
                 xs[e] = T(0);
         }
         if (REV && with_y) {
-            // ys[g][q] = ypad(top - 2 - q), q in [0, W + NP): the lagged outputs
-            // y[t-1-i] of the window's steps (y[-1-k] = zi[k])
             const T *yb = p.ysave + b * p.T;
             const T *zib = p.zi ? p.zi + b * N : nullptr;
-            constexpr int PY = W + NP;
-            for (int e = tid; e < Gb * PY; e += THREADS) {
+            for (int e = tid; e < Gc * PY; e += THREADS) {
                 const int g = e / PY;
-                const int q = e - g * PY;
-                const int64_t top = p.T - (tb + (int64_t)g * p.L + (int64_t)w * W);
-                const int64_t j = top - 2 - q;
+                const int r = e - g * PY;
+                int64_t row0;
+                int lo, hi;
+                rows(p, tb, Lc, g, w, row0, lo, hi);
+                const int64_t j = row0 - NP + r;
                 T *dst = ys + e;
-                if (j >= 0 && j < p.T)
+                if (j >= 0)  // j < top <= T
                     cp_async<sizeof(T)>(dst, yb + j);
-                else if (j < 0 && -1 - j < N && zib)
+                else if (-1 - j < N && zib)
                     *dst = zib[-1 - j];
                 else
                     *dst = T(0);
             }
         }
     }
+
+    __device__ static void load(const ChunkParams<T> &p, int64_t b, int64_t tb, int Gc, int Lc, int w, T *As,
+                                T *xs, T *ys, bool with_y) {
+        if (p.loader == kLoadVec)
+            load_vec(p, b, tb, Gc, Lc, w, As, xs, ys, with_y);
+        else
+            load_elem(p, b, tb, Gc, Lc, w, As, xs, ys, with_y);
+    }
 };
+
+// Phase A: NS steps of one window segment of a chunk-map lane (ring
+// positions U0..U0+NS-1), slots jbase.. of the window.
+template <typename T, int NP, bool REV, bool NEG, int WC, int U0, int NS>
+__device__ __forceinline__ void map_steps(const T *Ag, const T *xg, bool xlane, int jbase, T (&h)[NP]) {
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        const int u = (U0 + j) % NP;
+        const int jj = jbase + j;
+        const int slot = REV ? WC - 1 - jj : jj;
+        T a[NP];
+        lds_row<T, NP>(a, Ag + (size_t)slot * NP);
+        if constexpr (NEG) {
+#pragma unroll
+            for (int i = 0; i < NP; ++i) a[i] = -a[i];
+        }
+        const T in = xlane ? xg[slot] : T(0);
+        if constexpr (REV)
+            step_scatter<T, NP>(a, h, u, in);
+        else
+            h[u] = step_dot<T, NP>(a, h, u, in);
+    }
+}
+
+// Phase D: NS steps of the exact filter for one half-chunk, outputs to og.
+template <typename T, int NP, bool REV, bool NEG, int WC, int U0, int NS>
+__device__ __forceinline__ void fix_steps(const T *Ag, const T *xg, T *og, int jbase, T (&h)[NP]) {
+    T o[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        const int u = (U0 + j) % NP;
+        const int jj = jbase + j;
+        const int slot = REV ? WC - 1 - jj : jj;
+        T a[NP];
+        lds_row<T, NP>(a, Ag + (size_t)slot * NP);
+        if constexpr (NEG) {
+#pragma unroll
+            for (int i = 0; i < NP; ++i) a[i] = -a[i];
+        }
+        if constexpr (REV) {
+            o[j] = step_scatter<T, NP>(a, h, u, xg[slot]);
+        } else {
+            h[u] = step_dot<T, NP>(a, h, u, xg[slot]);
+            o[j] = h[u];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NS; ++j) og[jbase + j] = o[j];
+}
 
 // ----------------------------------------------------------------------------
 // The kernel.
@@ -337,31 +466,48 @@ struct Loader {
 template <typename T, int NP, bool REV, bool NEG>
 __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_kernel(ChunkParams<T> p) {
     constexpr int W = Cfg<NP>::W;
+    constexpr int WD = Cfg<NP>::WD;
     constexpr int THREADS = Cfg<NP>::THREADS;
     constexpr int V = 16 / sizeof(T);
-    constexpr int GS = group_stride(W, NP, sizeof(T));
+    constexpr int GSA = group_stride(W, NP, sizeof(T));
+    constexpr int GSD = group_stride(WD, NP, sizeof(T));
     constexpr int RS = map_row_stride(NP, sizeof(T));
     constexpr int MS = map_stride(NP, sizeof(T));
+    constexpr int PYD = WD + NP;
+    constexpr int PSE = agg_p_elems(NP, sizeof(T));
+    constexpr int ZSE = agg_z_elems(NP);
+    constexpr int HME = half_map_elems(NP, sizeof(T));
+    constexpr int KL = lookback_hops(NP, sizeof(T));
+    using LA = Loader<T, NP, REV, W>;
+    using LD = Loader<T, NP, REV, WD>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int N = p.N;
     const int G = p.G;
+    const int L = p.L;
+    const int LH = L / 2;  // phase D runs on half-chunks
     const int tid = threadIdx.x;
-    const SmemPlan S(sizeof(T), NP, W, G, N, REV);
+    const int lane = tid & 31;
+    const SmemPlan S(sizeof(T), NP, G, REV);
     T *Abuf = reinterpret_cast<T *>(smem + S.abuf);
     T *ibuf = reinterpret_cast<T *>(smem + S.ibuf);
     T *obuf = reinterpret_cast<T *>(smem + S.obuf);
     T *ybuf = reinterpret_cast<T *>(smem + S.ybuf);
     T *maps = reinterpret_cast<T *>(smem + S.maps);  // [Gp][NP rows of RS | z]
-    double *st = reinterpret_cast<double *>(smem + S.st);      // [Gp][NP]
-    double *s_in = reinterpret_cast<double *>(smem + S.sin);   // [NP]
+    T *lbP = reinterpret_cast<T *>(smem + S.lbP);    // [2][KL][PSE]
+    double *lbz = reinterpret_cast<double *>(smem + S.lbz);  // [2][KL][ZSE]
+    T *hmap = reinterpret_cast<T *>(smem + S.half);  // [G][HME]: first-half map, P[i][k] then z
+    double *st = reinterpret_cast<double *>(smem + S.st);    // [Gp][NP]
+    double *s_in = reinterpret_cast<double *>(smem + S.sin); // [NP]
     int64_t *misc = reinterpret_cast<int64_t *>(smem + S.misc);
     int Gp = 1;
     while (Gp < G) Gp <<= 1;
 
-    const bool vec = Loader<T, NP, REV>::fast(p);
     const int grp = tid / (N + 1);
     const int kk = tid - grp * (N + 1);
-    const int nwin = p.L / W;
+    const int nwin = L / W;  // windows per pass (phase D: the same count of WD-step windows)
+
+    // entries of the half maps beyond order N stay zero for the whole launch
+    for (int e = tid; e < G * HME; e += THREADS) hmap[e] = T(0);
 
     for (;;) {
         __syncthreads();
@@ -371,54 +517,51 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
         if (ticket >= p.nbatches) break;
         const int64_t kb = ticket / p.B;  // batch index within the signal
         const int64_t b = ticket - kb * p.B;
-        const int64_t tb = kb * (int64_t)G * p.L;  // first step of the batch
+        const int64_t tb = kb * (int64_t)G * L;  // first step of the batch
         const int64_t rem = p.T - tb;
-        const int Gb = (int)min64(G, (rem + p.L - 1) / p.L);
+        const int Gb = (int)min64(G, (rem + L - 1) / L);
 
         // ------------------------------------------------------------ phase A
         // chunk maps: N basis filters + one zero-state filter per chunk
-        if (N < NP)  // padded coefficient columns must read as zero
-            for (int e = tid; e < 2 * G * GS; e += THREADS)
-                if ((e % GS) % NP >= N) Abuf[e] = T(0);
+        if (p.loader == kLoadElem && N < NP)  // padded coefficient columns must read as zero
+            for (int e = tid; e < 2 * G * GSA; e += THREADS)
+                if ((e % GSA) % NP >= N) Abuf[e] = T(0);
         const bool active = grp < Gb;
         const bool xlane = (kk == N);
         T h[NP];
 #pragma unroll
         for (int j = 0; j < NP; ++j) h[j] = (active && !xlane && j == state_slot<REV, NP>(kk)) ? T(1) : T(0);
 
-        Loader<T, NP, REV>::load(p, vec, b, tb, Gb, 0, Abuf, ibuf, nullptr, false);
+        LA::load(p, b, tb, Gb, L, 0, Abuf, ibuf, nullptr, false);
         cp_async_commit();
         for (int w = 0; w < nwin; ++w) {
-            const T *As = Abuf + (size_t)(w & 1) * G * GS;
-            const T *xs = ibuf + (size_t)(w & 1) * G * W;
+            const int s = w & 1;
             if (w + 1 < nwin)
-                Loader<T, NP, REV>::load(p, vec, b, tb, Gb, w + 1, Abuf + (size_t)((w + 1) & 1) * G * GS,
-                                         ibuf + (size_t)((w + 1) & 1) * G * W, nullptr, false);
+                LA::load(p, b, tb, Gb, L, w + 1, Abuf + (size_t)(s ^ 1) * G * GSA, ibuf + (size_t)(s ^ 1) * G * W,
+                         nullptr, false);
             cp_async_commit();
             cp_async_wait<1>();
             __syncthreads();
             if (active) {
-                const T *Ag = As + (size_t)grp * GS;
-                const T *xg = xs + (size_t)grp * W;
-#pragma unroll 1
-                for (int blk = 0; blk < W / NP; ++blk) {
+                if (w == nwin / 2) {
+                    // the state after the first half of the chunk: column kk of
+                    // the half map (basis lanes) or its z (zero-state lane)
+                    T *Hg = hmap + (size_t)grp * HME;
 #pragma unroll
-                    for (int u = 0; u < NP; ++u) {
-                        const int j = blk * NP + u;
-                        const int slot = REV ? W - 1 - j : j;
-                        T a[NP];
-                        lds_row<T, NP>(a, Ag + (size_t)slot * NP);
-                        if constexpr (NEG) {
-#pragma unroll
-                            for (int i = 0; i < NP; ++i) a[i] = -a[i];
+                    for (int i = 0; i < NP; ++i) {
+                        if (i < N) {
+                            const T v = h[state_slot<REV, NP>(i)];
+                            if (!xlane)
+                                Hg[i * NP + kk] = v;
+                            else
+                                Hg[NP * NP + i] = v;
                         }
-                        const T in = xlane ? xg[slot] : T(0);
-                        if constexpr (REV)
-                            step_scatter<T, NP>(a, h, u, in);
-                        else
-                            h[u] = step_dot<T, NP>(a, h, u, in);
                     }
                 }
+                const T *Ag = Abuf + (size_t)s * G * GSA + (size_t)grp * GSA;
+                const T *xg = ibuf + (size_t)s * G * W + (size_t)grp * W;
+#pragma unroll 1
+                for (int blk = 0; blk < W / NP; ++blk) map_steps<T, NP, REV, NEG, W, 0, NP>(Ag, xg, xlane, blk * NP, h);
             }
             __syncthreads();
         }
@@ -501,19 +644,20 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                 s_in[tid] = v;
             }
         } else {
-            for (int e = tid; e < N * N; e += THREADS) {
-                const int r = e / N, c = e - (e / N) * N;
-                p.aggP[(size_t)me * N * N + e] = root[r * RS + c];
+            // padded record: rows/columns beyond N of the root are zero
+            for (int e = tid; e < PSE; e += THREADS) {
+                const int r = e / NP, c = e - (e / NP) * NP;
+                p.aggP[(size_t)me * PSE + e] = r < NP ? root[r * RS + c] : T(0);
             }
-            for (int e = tid; e < N; e += THREADS) p.aggz[(size_t)me * N + e] = (double)root[NP * RS + e];
+            for (int e = tid; e < ZSE; e += THREADS)
+                p.aggz[(size_t)me * ZSE + e] = e < NP ? (double)root[NP * RS + e] : 0.0;
             __threadfence();
             __syncthreads();
             if (tid == 0) st_release(p.flags + me, kFlagAgg);
             if (tid < 32) {
-                // warp 0: parallel look-back.  Lane l watches predecessor
+                // warp 0 alone: parallel look-back.  Lane l watches predecessor
                 // kb-1-l-32r; a round ends when every watched batch has
                 // published; the nearest inclusive state ends the walk.
-                const int lane = tid;
                 int64_t found = -1;
                 bool timeout = false;
                 for (int64_t hi = kb - 1; hi >= 0 && found < 0 && !timeout; hi -= 32) {
@@ -525,7 +669,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                         unsigned n = 0;
                         while (f == 0u) {
                             if (++n > p.spin_limit || ld_acquire(p.status) != 0u) {
-                                atomicOr(p.status, 1u);
+                                atomicOr(p.status, kStatusFlagWait);
                                 break;
                             }
                             __nanosleep(32);
@@ -537,81 +681,75 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                     if (inc) found = hi - (__ffs(inc) - 1);
                 }
                 if (found < 0 && !timeout) {  // cannot happen: batch 0 always publishes an inclusive state
-                    if (lane == 0) atomicOr(p.status, 2u);
+                    if (lane == 0) atomicOr(p.status, kStatusNoInclusive);
                     timeout = true;
                 }
                 // the flags seen above were acquired lane by lane; order every
                 // lane's reads of the predecessors' data after them
                 __threadfence();
-                if (timeout) {
-                    if (tid < NP) s_in[tid] = 0.0;
-                } else if (tid < NP) {
+                if (lane < NP) {
                     double v = 0.0;
-                    if (tid < N) v = p.incl[(size_t)(found * p.B + b) * N + tid];
-                    s_in[tid] = v;
+                    if (!timeout && lane < N) v = __ldcg(p.incl + (size_t)(found * p.B + b) * N + lane);
+                    s_in[lane] = v;
                 }
-                if (tid == 0) misc[1] = timeout ? -1 : found;
-            }
-            __syncthreads();
-            // compose the aggregates found+1 .. kb-1 in order.  The whole CTA
-            // streams them into a double-buffered shared stage, kLookbackChunk
-            // hops at a time, while warp 0 applies the previous stage.
-            const int64_t found = misc[1];
-            if (found >= 0) {
-                T *lbP = reinterpret_cast<T *>(smem + S.lbP);
-                double *lbz = reinterpret_cast<double *>(smem + S.lbz);
-                const int64_t m0 = found + 1;
-                const int64_t K = kb - m0;
-                const int64_t nch = (K + kLookbackChunk - 1) / kLookbackChunk;
-                const int per = N * N + N;
-                auto issue = [&](int64_t c) {
-                    const int64_t h0 = c * kLookbackChunk;
-                    const int nh = (int)min64(kLookbackChunk, K - h0);
-                    T *dP = lbP + (size_t)(c & 1) * kLookbackChunk * NP * NP;
-                    double *dz = lbz + (size_t)(c & 1) * kLookbackChunk * NP;
-                    for (int e = tid; e < nh * per; e += THREADS) {
-                        const int hh = e / per;
-                        const int r = e - hh * per;
-                        const int64_t idx = (m0 + h0 + hh) * p.B + b;
-                        if (r < N * N) {
-                            const int row = r / N, col = r - (r / N) * N;
-                            cp_async<sizeof(T)>(dP + (size_t)hh * NP * NP + row * NP + col,
-                                                p.aggP + (size_t)idx * N * N + r);
-                        } else {
-                            cp_async<8>(dz + (size_t)hh * NP + (r - N * N), p.aggz + (size_t)idx * N + (r - N * N));
-                        }
+                __syncwarp();
+                // compose the aggregates found+1 .. kb-1 in order.  They are
+                // staged KL at a time into a double-buffered shared
+                // stage with 16-byte cp.async (L2 only, so a line of a record
+                // published later is never served from this SM's L1); the next
+                // round is in flight while this one is applied.
+                constexpr int PV = PSE * (int)sizeof(T) / 16;  // vectors per P record
+                constexpr int ZV = ZSE * 8 / 16;               // vectors per z record
+                // lanes per row of the matvec: two for orders 8..16 (a shorter
+                // FMA chain per hop), one otherwise
+                constexpr int LPR = (NP >= 8 && NP <= 16) ? 2 : 1;
+                constexpr int CPL = NP / LPR;  // columns per lane
+                const int64_t first = timeout ? kb : found + 1;
+                const int nround = (int)((kb - first + KL - 1) / KL);
+                auto stage = [&](int r) {
+                    const int64_t m0 = first + (int64_t)r * KL;
+                    const int nh = (int)min64(KL, kb - m0);
+                    T *dP = lbP + (size_t)(r & 1) * KL * PSE;
+                    double *dz = lbz + (size_t)(r & 1) * KL * ZSE;
+                    for (int v = lane; v < nh * (PV + ZV); v += 32) {
+                        const int hh = v / (PV + ZV);
+                        const int q = v - hh * (PV + ZV);
+                        const int64_t idx = (m0 + hh) * p.B + b;
+                        if (q < PV)
+                            cp_async<16>(dP + (size_t)hh * PSE + q * (16 / sizeof(T)), p.aggP + (size_t)idx * PSE + q * (16 / sizeof(T)));
+                        else
+                            cp_async<16>(dz + (size_t)hh * ZSE + (q - PV) * 2, p.aggz + (size_t)idx * ZSE + (q - PV) * 2);
                     }
                 };
-                if (nch > 0) issue(0);
+                if (nround > 0) stage(0);
                 cp_async_commit();
-                for (int64_t c = 0; c < nch; ++c) {
-                    if (c + 1 < nch) issue(c + 1);
+                const int half = LPR == 2 ? lane >> 4 : 0;
+                const int row = LPR == 2 ? lane & 15 : lane;
+                const bool act = row < NP;
+                for (int r = 0; r < nround; ++r) {
+                    if (r + 1 < nround) stage(r + 1);
                     cp_async_commit();
                     cp_async_wait<1>();
-                    __syncthreads();
-                    if (tid < 32) {
-                        const int lane = tid;
-                        const int nh = (int)min64(kLookbackChunk, K - c * kLookbackChunk);
-                        const T *P0 = lbP + (size_t)(c & 1) * kLookbackChunk * NP * NP;
-                        const double *z0 = lbz + (size_t)(c & 1) * kLookbackChunk * NP;
-                        for (int hh = 0; hh < nh; ++hh) {
-                            double v = 0.0;
-                            if (lane < N) {
-                                const T *Pr = P0 + (size_t)hh * NP * NP + lane * NP;
-                                double v0 = z0[hh * NP + lane], v1 = 0.0;
+                    __syncwarp();
+                    const int nh = (int)min64(KL, kb - first - (int64_t)r * KL);
+                    const T *P0 = lbP + (size_t)(r & 1) * KL * PSE;
+                    const double *z0 = lbz + (size_t)(r & 1) * KL * ZSE;
+                    for (int hh = 0; hh < nh; ++hh) {
+                        double v = 0.0;
+                        if (act) {
+                            // padded rows and state entries are zero: no order guards
+                            const T *Pr = P0 + (size_t)hh * PSE + row * NP + half * CPL;
+                            const double *sv = s_in + half * CPL;
+                            double acc[4] = {half == 0 ? z0[hh * ZSE + row] : 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-                                for (int q = 0; q < NP; q += 2) {
-                                    if (q < N) v0 = fma((double)Pr[q], s_in[q], v0);
-                                    if (q + 1 < N) v1 = fma((double)Pr[q + 1], s_in[q + 1], v1);
-                                }
-                                v = v0 + v1;
-                            }
-                            __syncwarp();
-                            if (lane < N) s_in[lane] = v;
-                            __syncwarp();
+                            for (int q = 0; q < CPL; ++q) acc[q & 3] = fma((double)Pr[q], sv[q], acc[q & 3]);
+                            v = (acc[0] + acc[1]) + (acc[2] + acc[3]);
                         }
+                        if constexpr (LPR == 2) v += __shfl_xor_sync(0xffffffffu, v, 16);
+                        __syncwarp();
+                        if (act && half == 0) s_in[row] = v;
+                        __syncwarp();
                     }
-                    __syncthreads();
                 }
                 cp_async_wait<0>();
             }
@@ -661,63 +799,70 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
         }
 
         // ------------------------------------------------------------ phase D
-        // fix-up: one lane per chunk re-runs the chunk from its entry state
-        if (N < NP)
-            for (int e = tid; e < 2 * G * GS; e += THREADS)
-                if ((e % GS) % NP >= N) Abuf[e] = T(0);
-        const bool fix = tid < Gb;
+        // fix-up: one lane per half-chunk re-runs it from its exact entry
+        // state (second halves: the first half's map applied to the chunk's
+        // entry state, in FP64)
+        const int Gd = 2 * Gb;  // half-chunks of the batch
+        if (p.loader == kLoadElem && N < NP)
+            for (int e = tid; e < 2 * 2 * G * GSD; e += THREADS)
+                if ((e % GSD) % NP >= N) Abuf[e] = T(0);
+        const bool fix = tid < Gd;
+        {
+            const int g = tid >> 1;
+            const double *sg = st + (size_t)g * NP;
+            if (fix && (tid & 1)) {
+                const T *Hg = hmap + (size_t)g * HME;
 #pragma unroll
-        for (int i = 0; i < NP; ++i)
-            h[state_slot<REV, NP>(i)] = (fix && i < N) ? (T)st[(size_t)tid * NP + i] : T(0);
+                for (int i = 0; i < NP; ++i) {
+                    double v = (double)Hg[NP * NP + i];
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) v = fma((double)Hg[i * NP + k], sg[k], v);
+                    h[state_slot<REV, NP>(i)] = i < N ? (T)v : T(0);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < NP; ++i) h[state_slot<REV, NP>(i)] = (fix && i < N) ? (T)sg[i] : T(0);
+            }
+        }
         const bool ti = REV && p.gA && p.as_t == 0;
+        // grad_A rows are dense (B,T,N): 16-byte vectors when N fills NP
+        const bool gA_vec = N == NP && NP % V == 0 && is_aligned16<T>(p.gA);
         __syncthreads();
-        Loader<T, NP, REV>::load(p, vec, b, tb, Gb, 0, Abuf, ibuf, ybuf, REV);
+        LD::load(p, b, tb, Gd, LH, 0, Abuf, ibuf, ybuf, REV);
         cp_async_commit();
         for (int w = 0; w < nwin; ++w) {
-            const T *As = Abuf + (size_t)(w & 1) * G * GS;
-            const T *xs = ibuf + (size_t)(w & 1) * G * W;
-            const T *ys = ybuf + (size_t)(w & 1) * G * (W + NP);
+            const int s = w & 1;
             if (w + 1 < nwin)
-                Loader<T, NP, REV>::load(p, vec, b, tb, Gb, w + 1, Abuf + (size_t)((w + 1) & 1) * G * GS,
-                                         ibuf + (size_t)((w + 1) & 1) * G * W,
-                                         ybuf + (size_t)((w + 1) & 1) * G * (W + NP), REV);
+                LD::load(p, b, tb, Gd, LH, w + 1, Abuf + (size_t)(s ^ 1) * Gd * GSD, ibuf + (size_t)(s ^ 1) * Gd * WD,
+                         ybuf + (size_t)(s ^ 1) * Gd * PYD, REV);
             cp_async_commit();
             cp_async_wait<1>();
             __syncthreads();
+            const T *As = Abuf + (size_t)s * Gd * GSD;
+            const T *xs = ibuf + (size_t)s * Gd * WD;
+            const T *ys = ybuf + (size_t)s * Gd * PYD;
             if (fix) {
-                const T *Ag = As + (size_t)tid * GS;
-                const T *xg = xs + (size_t)tid * W;
-                T *og = obuf + (size_t)tid * W;
+                const T *Ag = As + (size_t)tid * GSD;
+                const T *xg = xs + (size_t)tid * WD;
+                T *og = obuf + (size_t)tid * WD;
+                if constexpr (WD % NP == 0) {
 #pragma unroll 1
-                for (int blk = 0; blk < W / NP; ++blk) {
-                    T o[NP];
-#pragma unroll
-                    for (int u = 0; u < NP; ++u) {
-                        const int j = blk * NP + u;
-                        const int slot = REV ? W - 1 - j : j;
-                        T a[NP];
-                        lds_row<T, NP>(a, Ag + (size_t)slot * NP);
-                        if constexpr (NEG) {
-#pragma unroll
-                            for (int i = 0; i < NP; ++i) a[i] = -a[i];
-                        }
-                        if constexpr (REV) {
-                            o[u] = step_scatter<T, NP>(a, h, u, xg[slot]);
-                        } else {
-                            h[u] = step_dot<T, NP>(a, h, u, xg[slot]);
-                            o[u] = h[u];
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < NP; ++u) og[blk * NP + u] = o[u];
+                    for (int blk = 0; blk < WD / NP; ++blk) fix_steps<T, NP, REV, NEG, WD, 0, NP>(Ag, xg, og, blk * NP, h);
+                } else {
+                    // NP == 2*WD: the ring advances by half a turn per window
+                    static_assert(NP == 2 * WD, "window/order mismatch");
+                    if (w & 1)
+                        fix_steps<T, NP, REV, NEG, WD, WD, WD>(Ag, xg, og, 0, h);
+                    else
+                        fix_steps<T, NP, REV, NEG, WD, 0, WD>(Ag, xg, og, 0, h);
                 }
             }
             __syncthreads();
-            // flush the window's outputs
-            for (int e = tid; e < Gb * W; e += THREADS) {
-                const int g = e / W;
-                const int j = e - g * W;
-                const int64_t pos = tb + (int64_t)g * p.L + (int64_t)w * W + j;  // step index
+            // flush the window's outputs (obuf is indexed by step)
+            for (int e = tid; e < Gd * WD; e += THREADS) {
+                const int g = e / WD;
+                const int j = e - g * WD;
+                const int64_t pos = tb + (int64_t)g * LH + (int64_t)w * WD + j;  // step index
                 if (pos < p.T) {
                     const int64_t t = REV ? p.T - 1 - pos : pos;
                     p.out[b * p.T + t] = obuf[e];
@@ -727,54 +872,42 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                 }
             }
             if (REV && p.gA) {
+                // row t = top-WD+rr of half-chunk g: grad_x[t] = obuf[g][WD-1-rr],
+                // y[t-1-i] = ys[g][rr+NP-1-i]
                 const T sgn = NEG ? T(1) : T(-1);
-                if (!ti && vec && NP % V == 0) {
-                    // rows t in [top-W, top-1] are contiguous: one 16-byte vector of
-                    // taps per thread and step
-                    constexpr int QR = NP / V;     // vectors per row
-                    constexpr int QPC = W * QR;    // vectors per chunk window
+                if (!ti && gA_vec) {
+                    // rows [top-WD, top) are contiguous in grad_A: one 16-byte
+                    // vector of taps per thread and row
+                    constexpr int QR = NP / V > 0 ? NP / V : 1;  // vectors per row (gA_vec: NP % V == 0)
+                    constexpr int QPC = WD * QR;                 // vectors per half-chunk window
                     using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-                    for (int e = tid; e < Gb * QPC; e += THREADS) {
+                    for (int e = tid; e < Gd * QPC; e += THREADS) {
                         const int g = e / QPC;
-                        const int remg = e - g * QPC;
-                        const int rr = remg / QR;  // row offset from the lowest time in the window
-                        const int i0 = (remg - rr * QR) * V;
-                        const int s = W - 1 - rr;
-                        const int64_t pos = tb + (int64_t)g * p.L + (int64_t)w * W + s;
-                        if (pos >= p.T) continue;
-                        const int64_t t = p.T - 1 - pos;
-                        const T gx = sgn * obuf[g * W + s];
-                        const T *yq = ys + g * (W + NP) + s + i0;
+                        const int v = e - g * QPC;
+                        const int rr = v / QR;
+                        const int i0 = (v - rr * QR) * V;
+                        const int64_t top = p.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
+                        const int64_t t = top - WD + rr;
+                        if (t < 0) continue;
+                        const T gx = sgn * obuf[g * WD + (WD - 1 - rr)];
+                        const T *yq = ys + g * PYD + rr + NP - 1 - i0;
                         VT o;
                         T *ov = reinterpret_cast<T *>(&o);
 #pragma unroll
-                        for (int j = 0; j < V; ++j) ov[j] = gx * yq[j];
+                        for (int j = 0; j < V; ++j) ov[j] = gx * yq[-j];
                         *reinterpret_cast<VT *>(p.gA + (b * p.T + t) * NP + i0) = o;
                     }
                 } else if (!ti) {
-                    const int per = W * N;
-                    for (int e = tid; e < Gb * per; e += THREADS) {
+                    const int per = WD * N;
+                    for (int e = tid; e < Gd * per; e += THREADS) {
                         const int g = e / per;
                         const int remg = e - g * per;
                         const int rr = remg / N;
                         const int i = remg - rr * N;
-                        const int s = W - 1 - rr;
-                        const int64_t pos = tb + (int64_t)g * p.L + (int64_t)w * W + s;
-                        if (pos >= p.T) continue;
-                        const int64_t t = p.T - 1 - pos;
-                        p.gA[(b * p.T + t) * N + i] = sgn * obuf[g * W + s] * ys[g * (W + NP) + s + i];
-                    }
-                } else {
-                    // time-invariant coefficients: per-thread partial sums per tap, added atomically
-                    for (int i = tid % NP; i < N; i += NP) {
-                        T acc = T(0);
-                        for (int e = tid / NP; e < Gb * W; e += THREADS / NP) {
-                            const int g = e / W;
-                            const int sl = e - g * W;
-                            const int64_t pos = tb + (int64_t)g * p.L + (int64_t)w * W + sl;
-                            if (pos < p.T) acc = fma(obuf[e], ys[g * (W + NP) + sl + i], acc);
-                        }
-                        if (acc != T(0)) atomicAdd(p.gA + b * N + i, sgn * acc);
+                        const int64_t top = p.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
+                        const int64_t t = top - WD + rr;
+                        if (t < 0) continue;
+                        p.gA[(b * p.T + t) * N + i] = sgn * obuf[g * WD + (WD - 1 - rr)] * ys[g * PYD + rr + NP - 1 - i];
                     }
                 }
             }
@@ -782,9 +915,9 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
         }
         cp_async_wait<0>();
         // grad_zi entries beyond the padded steps of the signal's last chunk are
-        // still pending in that chunk's exit state
-        if (REV && p.gzi && kb + 1 == p.nbps && tid == Gb - 1) {
-            const int64_t npad = tb + (int64_t)Gb * p.L - p.T;  // steps of the chunk with t < 0
+        // still pending in the exit state of its second half
+        if (REV && p.gzi && kb + 1 == p.nbps && tid == Gd - 1) {
+            const int64_t npad = tb + (int64_t)Gb * L - p.T;  // steps of the chunk with t < 0
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
                 const int64_t k = npad + i;
@@ -795,12 +928,80 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
 }
 
 // ----------------------------------------------------------------------------
+// Time-invariant coefficients: grad_a[b,i] = sgn * sum_t grad_x[b,t] *
+// ypad[b,t-1-i] with ypad(-1-k) = zi[b,k] (zero past k = N-1), from the
+// grad_x the chunked backward has written.  Block (x, b) reduces a strided
+// share of signal b and adds its per-tap sums atomically.
+// ----------------------------------------------------------------------------
+template <typename T, int NP>
+__global__ void __launch_bounds__(256) ti_grad_kernel(const T *gx, const T *y, const T *zi, T *ga, int64_t B,
+                                                     int64_t T_, int N, T sgn) {
+    __shared__ T part[8][NP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
+        const T *gb = gx + b * T_;
+        const T *yb = y + b * T_;
+        const T *zb = zi ? zi + b * N : nullptr;
+        T acc[NP];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) acc[i] = T(0);
+        for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T_;
+             t += (int64_t)gridDim.x * blockDim.x) {
+            const T g = gb[t];
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                if (i < N) {
+                    const int64_t j = t - 1 - i;
+                    const T yy = j >= 0 ? yb[j] : ((zb && i - t < N) ? zb[i - t] : T(0));
+                    acc[i] = fma(g, yy, acc[i]);
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+            T v = acc[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) part[warp][i] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < N && threadIdx.x < NP) {
+            T v = T(0);
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += part[w][threadIdx.x];
+            if (v != T(0)) atomicAdd(ga + b * N + threadIdx.x, sgn * v);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int NP>
+cudaError_t launch_ti_grad(const T *gx, const T *y, const T *zi, T *ga, int64_t B, int64_t T_, int N, bool neg,
+                           cudaStream_t st) {
+    const int64_t per_block = 256 * 64;  // samples a block covers per signal
+    const unsigned gxd = (unsigned)min64(4096, (T_ + per_block - 1) / per_block);
+    const unsigned gyd = (unsigned)min64(65535, B);
+    ti_grad_kernel<T, NP><<<dim3(gxd, gyd), 256, 0, st>>>(gx, y, zi, ga, B, T_, N, neg ? T(1) : T(-1));
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t ti_grad(const BwdArgs<T> &a, bool neg, int NP, cudaStream_t st) {
+    switch (NP) {
+#define LPCB_CASE(n) \
+    case n: return launch_ti_grad<T, n>(a.gx, a.y, a.zi, a.gA, a.B, a.T, (int)a.N, neg, st);
+        LPCB_FOR_EACH_NP(LPCB_CASE)
+#undef LPCB_CASE
+        default: return cudaErrorNotSupported;
+    }
+}
+
+// ----------------------------------------------------------------------------
 // Host side.
 // ----------------------------------------------------------------------------
-constexpr int kChunkLen = 128;   // target chunk length; rounded to a multiple of the window
+constexpr int kChunkLen = 256;   // target chunk length; rounded to an even number of windows
 constexpr int kMaxChunksPerBatch = 64;
 
-inline int threads_for(int) { return 256; }
+inline int threads_for(int) { return 256; }  // scan group: one group of N+1 lanes per chunk
 inline int window_for(int NP) { return NP * ((16 + NP - 1) / NP); }
 
 struct Plan {
@@ -809,16 +1010,18 @@ struct Plan {
 };
 
 // Chunks per batch: one group of N+1 lanes per chunk, capped so that the
-// backward's shared memory fits two CTAs per SM (fp32) or one (fp64).
+// shared memory of a CTA fits the occupancy the kernel is built for (fp32:
+// four CTAs per SM up to order 16, three above; fp64: two).
 inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N) {
     Plan pl;
     pl.NP = padded_order(N);
     const int W = window_for(pl.NP);
-    pl.L = W * ((kChunkLen + W - 1) / W);
+    pl.L = 2 * W * ((kChunkLen + 2 * W - 1) / (2 * W));  // an even number of windows: halves split on one
     int G = (int)(threads_for(pl.NP) / (N + 1));
     if (G > kMaxChunksPerBatch) G = kMaxChunksPerBatch;
-    const size_t budget = esz == 4 ? 110 * 1024 : 220 * 1024;
-    while (G > 1 && SmemPlan(esz, pl.NP, W, G, (int)N, true).total > budget) --G;
+    const int ctas = esz == 4 ? (pl.NP <= 16 ? 4 : 3) : 2;
+    const size_t budget = (size_t)228 * 1024 / ctas - 1024;  // per-SM shared memory less the per-CTA reserve
+    while (G > 1 && SmemPlan(esz, pl.NP, G, true).total > budget) --G;
     pl.G = G;
     const int64_t span = (int64_t)pl.G * pl.L;
     pl.nbps = (T + span - 1) / span;
@@ -827,10 +1030,26 @@ inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N) {
     return pl;
 }
 
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Whether windows can move as 16-byte vectors: dense rows of the padded
+// order, 16-byte rows and half windows, 16-byte aligned bases and signal
+// starts.
+template <typename T>
+bool vec_ok(const ChunkParams<T> &p, int NP) {
+    const size_t esz = sizeof(T);
+    const int WD = window_for(NP) / 2;
+    if (p.N != NP || p.as_t != NP || (NP * esz) % 16 != 0 || (WD * esz) % 16 != 0) return false;
+    if (!aligned16(p.A) || (p.as_b * esz) % 16 != 0) return false;
+    if (!aligned16(p.in) || (p.T * esz) % 16 != 0) return false;
+    if (p.ysave && !aligned16(p.ysave)) return false;
+    return true;
+}
+
 template <typename T, int NP, bool REV, bool NEG>
 cudaError_t launch_np(ChunkParams<T> p, cudaStream_t st) {
     auto kern = chunked_kernel<T, NP, REV, NEG>;
-    const SmemPlan S(sizeof(T), NP, Cfg<NP>::W, p.G, p.N, REV);
+    const SmemPlan S(sizeof(T), NP, p.G, REV);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S.total);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
@@ -841,6 +1060,7 @@ cudaError_t launch_np(ChunkParams<T> p, cudaStream_t st) {
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int64_t grid = (int64_t)sms * per_sm;
     if (grid > p.nbatches) grid = p.nbatches;
+    p.loader = vec_ok(p, NP) ? kLoadVec : kLoadElem;
     kern<<<(unsigned)grid, Cfg<NP>::THREADS, S.total, st>>>(p);
     return cudaGetLastError();
 }
@@ -940,7 +1160,9 @@ cudaError_t chunked_backward(const BwdArgs<T> &a, bool neg, void *ws, size_t ws_
     p.out = a.gx;
     p.gA = a.gA;
     p.gzi = a.gzi;
-    return neg ? dispatch<T, true, true>(p, pl.NP, st) : dispatch<T, true, false>(p, pl.NP, st);
+    e = neg ? dispatch<T, true, true>(p, pl.NP, st) : dispatch<T, true, false>(p, pl.NP, st);
+    if (e != cudaSuccess || !a.gA || a.a_stride_t != 0) return e;
+    return ti_grad<T>(a, neg, pl.NP, st);  // reads the grad_x just written
 }
 
 template cudaError_t chunked_forward<float>(const FwdArgs<float> &, bool, void *, size_t, cudaStream_t);
