@@ -110,6 +110,32 @@ int lpc_b200_forward_noalloc(int dtype, const void *x, const void *A,
                              void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Ragged batches.  No reference counterpart (the reference operators take a
+ * dense (B, T) batch; a ragged batch there is padded to the longest signal).
+ * nsig signals are concatenated along time: `offsets` is a DEVICE array of
+ * nsig+1 non-decreasing int64 sample offsets; signal s is samples
+ * [offsets[s], offsets[s+1]) of x, y, grad_y, grad_x and the same rows of A
+ * and grad_A (S rows of N, row stride N); zi and grad_zi are (nsig, N), zi
+ * may be NULL.  S = offsets[nsig] bounds the workspace.  One persistent launch
+ * covers every signal with the chunked scan; orders above 32 return
+ * LPC_ERR_UNSUPPORTED.  A negative signal length is treated as empty and
+ * recorded in the workspace status word.
+ * ------------------------------------------------------------------------- */
+size_t lpc_b200_ragged_workspace_size(int dtype, int64_t nsig, int64_t S, int64_t N);
+
+int lpc_b200_forward_ragged(int dtype, const void *x, const void *A,
+                            const int64_t *offsets, const void *zi, void *y,
+                            int64_t nsig, int64_t S, int64_t N, void *workspace,
+                            size_t workspace_bytes, void *stream);
+
+int lpc_b200_backward_ragged(int dtype, const void *grad_y, const void *A,
+                             const int64_t *offsets, const void *zi,
+                             const void *y, void *grad_x, void *grad_A,
+                             void *grad_zi, int64_t nsig, int64_t S, int64_t N,
+                             void *workspace, size_t workspace_bytes,
+                             void *stream);
+
+/* ---------------------------------------------------------------------------
  * Order-1 recurrence  out[t] = decay[t]*out[t-1] + impulse[t],  out[-1]=init.
  * Replaces the reference operator torchlpc::scan(impulse, decay, init)
  *   (torchlpc/csrc/scan_cpu.cpp:28-78,124-141; linear_recurrence.cu:232-291;

@@ -13,11 +13,11 @@ from typing import Optional, Tuple, Union
 import torch
 
 from ._ops import EXTENSION_LOADED, available_algos, get_algo, set_algo
-from .core import LPC
+from .core import LPC, LPCRagged
 from .recurrence import Recurrence
 
 __all__ = ["sample_wise_lpc", "linear_recurrence", "LPC", "Recurrence", "EXTENSION_LOADED",
-           "set_algo", "get_algo", "available_algos"]
+           "set_algo", "get_algo", "available_algos", "sample_wise_lpc_ragged", "LPCRagged"]
 
 
 def linear_recurrence(a: torch.Tensor, x: torch.Tensor, zi: Optional[torch.Tensor] = None) -> torch.Tensor:
@@ -97,3 +97,25 @@ def sample_wise_lpc(
     if return_zf:
         return y, y[:, -order:].flip(1)
     return y
+
+
+def sample_wise_lpc_ragged(
+    x: torch.Tensor,
+    a: torch.Tensor,
+    offsets: torch.Tensor,
+    zi: Optional[torch.Tensor] = None,
+) -> torch.Tensor:
+    """All-pole filtering of a ragged batch in one launch (no padding).
+
+    Signal s occupies samples ``offsets[s]:offsets[s+1]`` of x (S,) and rows of
+    a (S, N); zi (nsig, N) defaults to zeros.  Equivalent to running
+    ``sample_wise_lpc`` on each signal separately; orders up to 32.
+    """
+    assert x.ndim == 1 and a.ndim == 2 and a.shape[0] == x.shape[0]
+    assert offsets.ndim == 1 and offsets.dtype == torch.int64
+    nsig, order = offsets.shape[0] - 1, a.shape[1]
+    if zi is None:
+        zi = a.new_zeros(nsig, order)
+    else:
+        assert zi.shape == (nsig, order)
+    return LPCRagged.apply(x, a, offsets, zi)

@@ -66,3 +66,13 @@ def scan(impulse, decay, init):
 def scan_backward(grad_out, decay, init, out, need_decay, need_init):
     _require()
     return torch.ops.torchlpc_b200.scan_backward(grad_out, decay, init, out, need_decay, need_init, _algo)
+
+
+def lpc_ragged(x, A, offsets, zi):
+    _require()
+    return torch.ops.torchlpc_b200.lpc_ragged(x, A, offsets, zi)
+
+
+def lpc_backward_ragged(grad_y, A, offsets, zi, y, need_A, need_zi):
+    _require()
+    return torch.ops.torchlpc_b200.lpc_backward_ragged(grad_y, A, offsets, zi, y, need_A, need_zi)

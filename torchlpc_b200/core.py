@@ -94,3 +94,31 @@ class LPC(Function):
         x, A, zi = (t.reshape(-1, *t.shape[2:]) for t in map(front, args, in_dims))
         y = LPC.apply(x, A, zi)
         return y.reshape(info.batch_size, -1, *y.shape[1:]), 0
+
+
+class LPCRagged(Function):
+    """The all-pole filter over a ragged batch: signals concatenated along time.
+
+    ``LPCRagged.apply(x, A, offsets, zi)`` with x (S,), A (S,N), offsets
+    (nsig+1,) int64 on x's device (signal s is samples offsets[s] to
+    offsets[s+1]) and zi (nsig,N).  No counterpart in the reference, which
+    filters a dense (B,T) batch (torchlpc/core.py:159-229).  The backward is
+    the fused CUDA kernel; it is not itself differentiable.
+    """
+
+    @staticmethod
+    def forward(x: torch.Tensor, A: torch.Tensor, offsets: torch.Tensor, zi: torch.Tensor) -> torch.Tensor:
+        return _ops.lpc_ragged(x, A, offsets, zi)
+
+    @staticmethod
+    def setup_context(ctx: Any, inputs: List[Any], output: Any) -> Any:
+        _, A, offsets, zi = inputs
+        ctx.save_for_backward(A, offsets, zi, output)
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx: Any, grad_y: torch.Tensor):
+        A, offsets, zi, y = ctx.saved_tensors
+        needs = ctx.needs_input_grad
+        gx, gA, gzi = _ops.lpc_backward_ragged(grad_y, A, offsets, zi, y, bool(needs[1]), bool(needs[3]))
+        return (gx if needs[0] else None, gA if needs[1] else None, None, gzi if needs[3] else None)

@@ -127,6 +127,66 @@ int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A, co
                               a_stride_b, a_stride_t, workspace, workspace_bytes, s);
 }
 
+size_t lpc_b200_ragged_workspace_size(int dtype, int64_t nsig, int64_t S, int64_t N) {
+    if (!dtype_ok(dtype) || nsig < 0 || S < 0 || N < 1 || N > kMaxOrder) return 0;
+    if (!chunked_supported(N) || nsig == 0) return 0;
+    return chunked_ragged_workspace(dtype == LPC_F32 ? 4 : 8, nsig, S, N);
+}
+
+namespace {
+int ragged_check(int dtype, const int64_t *offsets, int64_t nsig, int64_t S, int64_t N, void *ws,
+                 size_t wsb) {
+    if (!dtype_ok(dtype) || nsig < 0 || S < 0 || N < 1 || N > kMaxOrder || nsig >= (int64_t(1) << 31))
+        return LPC_ERR_INVALID_ARGUMENT;
+    if (nsig > 0 && !offsets) return LPC_ERR_INVALID_ARGUMENT;
+    if (!chunked_supported(N)) return LPC_ERR_UNSUPPORTED;
+    if (nsig > 0 && (!ws || wsb < chunked_ragged_workspace(dtype == LPC_F32 ? 4 : 8, nsig, S, N)))
+        return LPC_ERR_WORKSPACE;
+    return LPC_OK;
+}
+}  // namespace
+
+int lpc_b200_forward_ragged(int dtype, const void *x, const void *A, const int64_t *offsets,
+                            const void *zi, void *y, int64_t nsig, int64_t S, int64_t N,
+                            void *workspace, size_t workspace_bytes, void *stream) {
+    const int rc = ragged_check(dtype, offsets, nsig, S, N, workspace, workspace_bytes);
+    if (rc != LPC_OK) return rc;
+    if (nsig == 0) return LPC_OK;
+    if (S > 0 && (!x || !A || !y)) return LPC_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == LPC_F32)
+        return cuda_status(chunked_forward_ragged<float>(
+            static_cast<const float *>(x), static_cast<const float *>(A), offsets,
+            static_cast<const float *>(zi), static_cast<float *>(y), nsig, S, N, workspace,
+            workspace_bytes, s));
+    return cuda_status(chunked_forward_ragged<double>(
+        static_cast<const double *>(x), static_cast<const double *>(A), offsets,
+        static_cast<const double *>(zi), static_cast<double *>(y), nsig, S, N, workspace,
+        workspace_bytes, s));
+}
+
+int lpc_b200_backward_ragged(int dtype, const void *grad_y, const void *A, const int64_t *offsets,
+                             const void *zi, const void *y, void *grad_x, void *grad_A,
+                             void *grad_zi, int64_t nsig, int64_t S, int64_t N, void *workspace,
+                             size_t workspace_bytes, void *stream) {
+    const int rc = ragged_check(dtype, offsets, nsig, S, N, workspace, workspace_bytes);
+    if (rc != LPC_OK) return rc;
+    if (nsig == 0) return LPC_OK;
+    if (S > 0 && (!grad_y || !A || !y || !grad_x)) return LPC_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == LPC_F32)
+        return cuda_status(chunked_backward_ragged<float>(
+            static_cast<const float *>(grad_y), static_cast<const float *>(A), offsets,
+            static_cast<const float *>(zi), static_cast<const float *>(y),
+            static_cast<float *>(grad_x), static_cast<float *>(grad_A), static_cast<float *>(grad_zi),
+            nsig, S, N, workspace, workspace_bytes, s));
+    return cuda_status(chunked_backward_ragged<double>(
+        static_cast<const double *>(grad_y), static_cast<const double *>(A), offsets,
+        static_cast<const double *>(zi), static_cast<const double *>(y),
+        static_cast<double *>(grad_x), static_cast<double *>(grad_A), static_cast<double *>(grad_zi),
+        nsig, S, N, workspace, workspace_bytes, s));
+}
+
 size_t lpc_b200_scan_workspace_size(int dtype, int algo, int64_t B, int64_t T) {
     if (!dtype_ok(dtype) || !sizes_ok(B, T, 1)) return 0;
     if (resolve_algo(algo, B, T, 1, 1) != LPC_ALGO_CHUNKED) return 0;

@@ -122,11 +122,25 @@ struct ChunkParams {
     int loader;      // window loader: kLoadElem or kLoadVec
     int64_t nbps;    // batches per signal
     int64_t nbatches;
+    const int64_t *roff;  // ragged: signal offsets (nsig+1) into x/y (nullptr: uniform B x T)
+    int64_t *bb;          // ragged: first batch of each signal (nsig+1, in the workspace)
+    int64_t nsig;
     unsigned *counter, *status, *flags;
     F *aggP;         // [nbatches][agg_p_elems]
     double *aggz;    // [nbatches][agg_z_elems]
     double *incl;    // [nbatches][N]
     unsigned spin_limit;
+};
+
+// The signal a batch belongs to.
+struct Sig {
+    int64_t T;       // samples
+    int64_t xo;      // offset of sample 0 in x, y, grad_y, grad_x (grad_A rows: xo * N)
+    int64_t ao;      // offset of row 0 in A
+    int64_t zo;      // offset in zi and grad_zi
+    int64_t kb, nb;  // this batch's index within the signal, batches of the signal
+    int64_t fb, fs;  // workspace index of batch m of the signal: fb + m * fs
+    int vx;          // input windows move as 16-byte vectors
 };
 
 template <int NP>
@@ -248,8 +262,8 @@ struct SmemPlan {
         off += al((size_t)Gp * NP * sizeof(double));
         sin = off;
         off += al((size_t)NP * sizeof(double));
-        misc = off;  // ticket
-        off += 64;
+        misc = off;  // ticket, the batch's signal
+        off += 128;
         total = off;
     }
 };
@@ -277,14 +291,14 @@ struct Loader {
     static constexpr int PY = WC + NP;
 
     // First row held by slot 0 of chunk g's window w, and the valid slot range.
-    __device__ static void rows(const ChunkParams<T> &p, int64_t tb, int Lc, int g, int w, int64_t &row0,
-                                int &lo, int &hi) {
+    __device__ static void rows(const Sig &sg, int64_t tb, int Lc, int g, int w, int64_t &row0, int &lo,
+                                int &hi) {
         if (!REV) {
             row0 = tb + (int64_t)g * Lc + (int64_t)w * WC;
             lo = 0;
-            hi = (int)max64(0, min64(WC, p.T - row0));
+            hi = (int)max64(0, min64(WC, sg.T - row0));
         } else {
-            const int64_t top = p.T - (tb + (int64_t)g * Lc + (int64_t)w * WC);
+            const int64_t top = sg.T - (tb + (int64_t)g * Lc + (int64_t)w * WC);
             row0 = top - WC;
             lo = (int)min64(WC, max64(0, -row0));
             hi = WC;
@@ -293,23 +307,23 @@ struct Loader {
 
     // Vector path: all threads, one 16-byte cp.async per vector of a chunk's
     // rows, inputs and lagged outputs.  The caller commits the group.
-    __device__ static void load_vec(const ChunkParams<T> &p, int64_t b, int64_t tb, int Gc, int Lc, int w,
+    __device__ static void load_vec(const ChunkParams<T> &p, const Sig &sg, int64_t tb, int Gc, int Lc, int w,
                                     T *As, T *xs, T *ys, bool with_y) {
         constexpr int V = 16 / sizeof(T);
         constexpr int RV = NP / V > 0 ? NP / V : 1;  // vectors per row
         constexpr int AV = WC * RV;                  // coefficient vectors per chunk window
         constexpr int XV = WC / V > 0 ? WC / V : 1;  // input vectors
         constexpr int YV = PY / V;                   // lagged-output vectors
-        const int per = AV + XV + ((REV && with_y) ? YV : 0);
+        const int per = AV + (xs ? XV + ((REV && with_y) ? YV : 0) : 0);  // rows only when xs is null
         const int tid = threadIdx.x;
-        const T *Ab = p.A + b * p.as_b;
-        const T *inb = p.in + b * p.T;
+        const T *Ab = p.A + sg.ao;
+        const T *inb = p.in + sg.xo;
         for (int e = tid; e < Gc * per; e += THREADS) {
             const int g = e / per;
             const int q = e - g * per;
             int64_t row0;
             int lo, hi;
-            rows(p, tb, Lc, g, w, row0, lo, hi);
+            rows(sg, tb, Lc, g, w, row0, lo, hi);
             if (q < AV) {
                 const int r = q / RV;
                 T *dst = As + (size_t)g * GS + q * V;
@@ -333,9 +347,9 @@ struct Loader {
                 T *dst = ys + (size_t)g * PY + r;
                 const int64_t j0 = row0 - NP + r;  // a multiple of V: all or none of the vector is before t = 0
                 if (j0 >= 0) {
-                    cp_async<16>(dst, p.ysave + b * p.T + j0);
+                    cp_async<16>(dst, p.ysave + sg.xo + j0);
                 } else {
-                    const T *zib = p.zi ? p.zi + b * p.N : nullptr;
+                    const T *zib = p.zi ? p.zi + sg.zo : nullptr;
 #pragma unroll
                     for (int j = 0; j < V; ++j) {
                         const int64_t k = -1 - (j0 + j);
@@ -348,21 +362,21 @@ struct Loader {
 
     // Element path: all threads, one cp.async per element (any stride and
     // alignment).  The caller commits the group.
-    __device__ static void load_elem(const ChunkParams<T> &p, int64_t b, int64_t tb, int Gc, int Lc, int w,
-                                     T *As, T *xs, T *ys, bool with_y) {
+    __device__ static void load_elem(const ChunkParams<T> &p, const Sig &sg, int64_t tb, int Gc, int Lc, int w,
+                                     T *As, T *xs, T *ys, bool with_y, bool rows_too) {
         const int N = p.N;
         const int tid = threadIdx.x;
-        const T *Ab = p.A + b * p.as_b;
-        const T *inb = p.in + b * p.T;
+        const T *Ab = p.A + sg.ao;
+        const T *inb = p.in + sg.xo;
         const int per = WC * N;
-        for (int e = tid; e < Gc * per; e += THREADS) {
+        for (int e = tid; rows_too && e < Gc * per; e += THREADS) {
             const int g = e / per;
             const int rem = e - g * per;
             const int r = rem / N;
             const int i = rem - r * N;
             int64_t row0;
             int lo, hi;
-            rows(p, tb, Lc, g, w, row0, lo, hi);
+            rows(sg, tb, Lc, g, w, row0, lo, hi);
             T *dst = As + (size_t)g * GS + r * NP + i;
             if (r >= lo && r < hi)
                 cp_async<sizeof(T)>(dst, Ab + (row0 + r) * p.as_t + i);
@@ -375,21 +389,21 @@ struct Loader {
             const int r = e - g * WC;
             int64_t row0;
             int lo, hi;
-            rows(p, tb, Lc, g, w, row0, lo, hi);
+            rows(sg, tb, Lc, g, w, row0, lo, hi);
             if (r >= lo && r < hi)
                 cp_async<sizeof(T)>(xs + e, inb + row0 + r);
             else
                 xs[e] = T(0);
         }
         if (REV && with_y) {
-            const T *yb = p.ysave + b * p.T;
-            const T *zib = p.zi ? p.zi + b * N : nullptr;
+            const T *yb = p.ysave + sg.xo;
+            const T *zib = p.zi ? p.zi + sg.zo : nullptr;
             for (int e = tid; e < Gc * PY; e += THREADS) {
                 const int g = e / PY;
                 const int r = e - g * PY;
                 int64_t row0;
                 int lo, hi;
-                rows(p, tb, Lc, g, w, row0, lo, hi);
+                rows(sg, tb, Lc, g, w, row0, lo, hi);
                 const int64_t j = row0 - NP + r;
                 T *dst = ys + e;
                 if (j >= 0)  // j < top <= T
@@ -402,12 +416,18 @@ struct Loader {
         }
     }
 
-    __device__ static void load(const ChunkParams<T> &p, int64_t b, int64_t tb, int Gc, int Lc, int w, T *As,
+    // Vector rows and inputs when both allow it; vector rows with element
+    // inputs when only the signal start or length is unaligned.
+    __device__ static void load(const ChunkParams<T> &p, const Sig &sg, int64_t tb, int Gc, int Lc, int w, T *As,
                                 T *xs, T *ys, bool with_y) {
-        if (p.loader == kLoadVec)
-            load_vec(p, b, tb, Gc, Lc, w, As, xs, ys, with_y);
-        else
-            load_elem(p, b, tb, Gc, Lc, w, As, xs, ys, with_y);
+        if (p.loader == kLoadVec && sg.vx) {
+            load_vec(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y);
+        } else if (p.loader == kLoadVec) {
+            load_vec(p, sg, tb, Gc, Lc, w, As, nullptr, nullptr, false);
+            load_elem(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y, false);
+        } else {
+            load_elem(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y, true);
+        }
     }
 };
 
@@ -505,20 +525,62 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
     const int grp = tid / (N + 1);
     const int kk = tid - grp * (N + 1);
     const int nwin = L / W;  // windows per pass (phase D: the same count of WD-step windows)
+    const int64_t nbatches = p.roff ? p.bb[p.nsig] : p.nbatches;
+    Sig *sgs = reinterpret_cast<Sig *>(misc + 1);
 
     // entries of the half maps beyond order N stay zero for the whole launch
     for (int e = tid; e < G * HME; e += THREADS) hmap[e] = T(0);
 
     for (;;) {
         __syncthreads();
-        if (tid == 0) misc[0] = (int64_t)atomicAdd(p.counter, 1u);
+        if (tid == 0) {
+            const int64_t t = (int64_t)atomicAdd(p.counter, 1u);
+            misc[0] = t;
+            if (t < nbatches) {
+                Sig q;
+                if (p.roff) {
+                    // ragged: batches are numbered signal by signal; find the
+                    // signal whose range of batches holds the ticket
+                    int64_t lo = 0, hi = p.nsig;  // bb[lo] <= t < bb[hi]
+                    while (hi - lo > 1) {
+                        const int64_t mid = (lo + hi) / 2;
+                        if (p.bb[mid] <= t) lo = mid; else hi = mid;
+                    }
+                    q.T = p.roff[lo + 1] - p.roff[lo];
+                    q.xo = p.roff[lo];
+                    q.ao = p.roff[lo] * p.as_t;
+                    q.zo = lo * N;
+                    q.kb = t - p.bb[lo];
+                    q.nb = p.bb[lo + 1] - p.bb[lo];
+                    q.fb = p.bb[lo];
+                    q.fs = 1;
+                } else {
+                    // uniform: batch kb of every signal before batch kb+1 of any
+                    const int64_t b = t % p.B;
+                    q.T = p.T;
+                    q.xo = b * p.T;
+                    q.ao = b * p.as_b;
+                    q.zo = b * N;
+                    q.kb = t / p.B;
+                    q.nb = p.nbps;
+                    q.fb = b;
+                    q.fs = p.B;
+                }
+                // vector input windows need an aligned signal start and a
+                // length of whole vectors: backward windows start at T - pos,
+                // and a window's last vector must not reach past the signal
+                q.vx = (WD * (int)sizeof(T)) % 16 == 0 && (q.T * (int64_t)sizeof(T)) % 16 == 0 &&
+                       is_aligned16<T>(p.in + q.xo) && (!p.ysave || is_aligned16<T>(p.ysave + q.xo));
+                *sgs = q;
+            }
+        }
         __syncthreads();
         const int64_t ticket = misc[0];
-        if (ticket >= p.nbatches) break;
-        const int64_t kb = ticket / p.B;  // batch index within the signal
-        const int64_t b = ticket - kb * p.B;
+        if (ticket >= nbatches) break;
+        const Sig sg = *sgs;
+        const int64_t kb = sg.kb;  // batch index within the signal
         const int64_t tb = kb * (int64_t)G * L;  // first step of the batch
-        const int64_t rem = p.T - tb;
+        const int64_t rem = sg.T - tb;
         const int Gb = (int)min64(G, (rem + L - 1) / L);
 
         // ------------------------------------------------------------ phase A
@@ -532,12 +594,12 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
 #pragma unroll
         for (int j = 0; j < NP; ++j) h[j] = (active && !xlane && j == state_slot<REV, NP>(kk)) ? T(1) : T(0);
 
-        LA::load(p, b, tb, Gb, L, 0, Abuf, ibuf, nullptr, false);
+        LA::load(p, sg, tb, Gb, L, 0, Abuf, ibuf, nullptr, false);
         cp_async_commit();
         for (int w = 0; w < nwin; ++w) {
             const int s = w & 1;
             if (w + 1 < nwin)
-                LA::load(p, b, tb, Gb, L, w + 1, Abuf + (size_t)(s ^ 1) * G * GSA, ibuf + (size_t)(s ^ 1) * G * W,
+                LA::load(p, sg, tb, Gb, L, w + 1, Abuf + (size_t)(s ^ 1) * G * GSA, ibuf + (size_t)(s ^ 1) * G * W,
                          nullptr, false);
             cp_async_commit();
             cp_async_wait<1>();
@@ -640,7 +702,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
         if (kb == 0) {
             if (tid < NP) {
                 double v = 0.0;
-                if (!REV && p.zi && tid < N) v = (double)p.zi[b * N + tid];
+                if (!REV && p.zi && tid < N) v = (double)p.zi[sg.zo + tid];
                 s_in[tid] = v;
             }
         } else {
@@ -664,7 +726,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                     const int64_t m = hi - lane;
                     unsigned f = kFlagInc;  // batches before 0 do not exist: treat as resolved
                     if (m >= 0) {
-                        const unsigned *fp = p.flags + m * p.B + b;
+                        const unsigned *fp = p.flags + sg.fb + m * sg.fs;
                         f = ld_acquire(fp);
                         unsigned n = 0;
                         while (f == 0u) {
@@ -689,7 +751,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                 __threadfence();
                 if (lane < NP) {
                     double v = 0.0;
-                    if (!timeout && lane < N) v = __ldcg(p.incl + (size_t)(found * p.B + b) * N + lane);
+                    if (!timeout && lane < N) v = __ldcg(p.incl + (size_t)(sg.fb + found * sg.fs) * N + lane);
                     s_in[lane] = v;
                 }
                 __syncwarp();
@@ -714,7 +776,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                     for (int v = lane; v < nh * (PV + ZV); v += 32) {
                         const int hh = v / (PV + ZV);
                         const int q = v - hh * (PV + ZV);
-                        const int64_t idx = (m0 + hh) * p.B + b;
+                        const int64_t idx = sg.fb + (m0 + hh) * sg.fs;
                         if (q < PV)
                             cp_async<16>(dP + (size_t)hh * PSE + q * (16 / sizeof(T)), p.aggP + (size_t)idx * PSE + q * (16 / sizeof(T)));
                         else
@@ -756,7 +818,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
         }
         __syncthreads();
         // inclusive state of this batch: root applied to s_in
-        if (kb + 1 < p.nbps) {
+        if (kb + 1 < sg.nb) {
             if (tid < N) {
                 double v = (double)root[NP * RS + tid];
                 for (int q = 0; q < N; ++q) v = fma((double)root[tid * RS + q], s_in[q], v);
@@ -828,12 +890,12 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
         // grad_A rows are dense (B,T,N): 16-byte vectors when N fills NP
         const bool gA_vec = N == NP && NP % V == 0 && is_aligned16<T>(p.gA);
         __syncthreads();
-        LD::load(p, b, tb, Gd, LH, 0, Abuf, ibuf, ybuf, REV);
+        LD::load(p, sg, tb, Gd, LH, 0, Abuf, ibuf, ybuf, REV);
         cp_async_commit();
         for (int w = 0; w < nwin; ++w) {
             const int s = w & 1;
             if (w + 1 < nwin)
-                LD::load(p, b, tb, Gd, LH, w + 1, Abuf + (size_t)(s ^ 1) * Gd * GSD, ibuf + (size_t)(s ^ 1) * Gd * WD,
+                LD::load(p, sg, tb, Gd, LH, w + 1, Abuf + (size_t)(s ^ 1) * Gd * GSD, ibuf + (size_t)(s ^ 1) * Gd * WD,
                          ybuf + (size_t)(s ^ 1) * Gd * PYD, REV);
             cp_async_commit();
             cp_async_wait<1>();
@@ -863,12 +925,12 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                 const int g = e / WD;
                 const int j = e - g * WD;
                 const int64_t pos = tb + (int64_t)g * LH + (int64_t)w * WD + j;  // step index
-                if (pos < p.T) {
-                    const int64_t t = REV ? p.T - 1 - pos : pos;
-                    p.out[b * p.T + t] = obuf[e];
-                } else if (REV && p.gzi && pos - p.T < N) {
+                if (pos < sg.T) {
+                    const int64_t t = REV ? sg.T - 1 - pos : pos;
+                    p.out[sg.xo + t] = obuf[e];
+                } else if (REV && p.gzi && pos - sg.T < N) {
                     // steps past t = 0 carry the adjoint into the initial conditions
-                    p.gzi[b * N + (pos - p.T)] = obuf[e];
+                    p.gzi[sg.zo + (pos - sg.T)] = obuf[e];
                 }
             }
             if (REV && p.gA) {
@@ -886,7 +948,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                         const int v = e - g * QPC;
                         const int rr = v / QR;
                         const int i0 = (v - rr * QR) * V;
-                        const int64_t top = p.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
+                        const int64_t top = sg.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
                         const int64_t t = top - WD + rr;
                         if (t < 0) continue;
                         const T gx = sgn * obuf[g * WD + (WD - 1 - rr)];
@@ -895,7 +957,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                         T *ov = reinterpret_cast<T *>(&o);
 #pragma unroll
                         for (int j = 0; j < V; ++j) ov[j] = gx * yq[-j];
-                        *reinterpret_cast<VT *>(p.gA + (b * p.T + t) * NP + i0) = o;
+                        *reinterpret_cast<VT *>(p.gA + (sg.xo + t) * NP + i0) = o;
                     }
                 } else if (!ti) {
                     const int per = WD * N;
@@ -904,10 +966,10 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
                         const int remg = e - g * per;
                         const int rr = remg / N;
                         const int i = remg - rr * N;
-                        const int64_t top = p.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
+                        const int64_t top = sg.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
                         const int64_t t = top - WD + rr;
                         if (t < 0) continue;
-                        p.gA[(b * p.T + t) * N + i] = sgn * obuf[g * WD + (WD - 1 - rr)] * ys[g * PYD + rr + NP - 1 - i];
+                        p.gA[(sg.xo + t) * N + i] = sgn * obuf[g * WD + (WD - 1 - rr)] * ys[g * PYD + rr + NP - 1 - i];
                     }
                 }
             }
@@ -916,12 +978,12 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
         cp_async_wait<0>();
         // grad_zi entries beyond the padded steps of the signal's last chunk are
         // still pending in the exit state of its second half
-        if (REV && p.gzi && kb + 1 == p.nbps && tid == Gd - 1) {
-            const int64_t npad = tb + (int64_t)Gb * L - p.T;  // steps of the chunk with t < 0
+        if (REV && p.gzi && kb + 1 == sg.nb && tid == Gd - 1) {
+            const int64_t npad = tb + (int64_t)Gb * L - sg.T;  // steps of the chunk with t < 0
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
                 const int64_t k = npad + i;
-                if (i < N && k < N) p.gzi[b * N + k] = h[state_slot<REV, NP>(i)];
+                if (i < N && k < N) p.gzi[sg.zo + k] = h[state_slot<REV, NP>(i)];
             }
         }
     }
@@ -1032,18 +1094,14 @@ inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N) {
 
 inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-// Whether windows can move as 16-byte vectors: dense rows of the padded
-// order, 16-byte rows and half windows, 16-byte aligned bases and signal
-// starts.
+// Whether coefficient rows can move as 16-byte vectors: dense rows of the
+// padded order, 16-byte rows, 16-byte aligned base and signal strides.  (Input
+// windows are checked per batch: ragged signals start anywhere.)
 template <typename T>
 bool vec_ok(const ChunkParams<T> &p, int NP) {
     const size_t esz = sizeof(T);
-    const int WD = window_for(NP) / 2;
-    if (p.N != NP || p.as_t != NP || (NP * esz) % 16 != 0 || (WD * esz) % 16 != 0) return false;
-    if (!aligned16(p.A) || (p.as_b * esz) % 16 != 0) return false;
-    if (!aligned16(p.in) || (p.T * esz) % 16 != 0) return false;
-    if (p.ysave && !aligned16(p.ysave)) return false;
-    return true;
+    if (p.N != NP || p.as_t != NP || (NP * esz) % 16 != 0) return false;
+    return aligned16(p.A) && (p.as_b * esz) % 16 == 0;
 }
 
 template <typename T, int NP, bool REV, bool NEG>
@@ -1059,7 +1117,7 @@ cudaError_t launch_np(ChunkParams<T> p, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int64_t grid = (int64_t)sms * per_sm;
-    if (grid > p.nbatches) grid = p.nbatches;
+    if (grid > p.nbatches) grid = p.nbatches;  // ragged: an upper bound on the batches
     p.loader = vec_ok(p, NP) ? kLoadVec : kLoadElem;
     kern<<<(unsigned)grid, Cfg<NP>::THREADS, S.total, st>>>(p);
     return cudaGetLastError();
@@ -1164,6 +1222,148 @@ cudaError_t chunked_backward(const BwdArgs<T> &a, bool neg, void *ws, size_t ws_
     if (e != cudaSuccess || !a.gA || a.a_stride_t != 0) return e;
     return ti_grad<T>(a, neg, pl.NP, st);  // reads the grad_x just written
 }
+
+// ----------------------------------------------------------------------------
+// Ragged batches: nsig signals concatenated along time, signal s occupying
+// samples [off[s], off[s+1]) of x / y and rows of A (S, N); zi (nsig, N).
+// Batches are numbered signal by signal, so the workspace needs at most
+// nsig + S / span + 1 batch records; the first batch of each signal (bb) is
+// computed on the device from the offsets.
+// ----------------------------------------------------------------------------
+namespace {
+
+constexpr unsigned kStatusBadOffsets = 8u;  // a signal with a negative length (treated as empty)
+
+__global__ void __launch_bounds__(1024) batch_base_kernel(const int64_t *off, int64_t nsig, int64_t span,
+                                                          int64_t *bb, unsigned *status) {
+    __shared__ int64_t sh[1024];
+    __shared__ int64_t carry;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        carry = 0;
+        bb[0] = 0;
+    }
+    __syncthreads();
+    for (int64_t base = 0; base < nsig; base += 1024) {
+        const int64_t s = base + tid;
+        int64_t v = 0;
+        if (s < nsig) {
+            int64_t len = off[s + 1] - off[s];
+            if (len < 0) {
+                atomicOr(status, kStatusBadOffsets);
+                len = 0;
+            }
+            v = (len + span - 1) / span;
+        }
+        sh[tid] = v;
+        __syncthreads();
+        for (int d = 1; d < 1024; d <<= 1) {  // inclusive scan of the batch counts
+            const int64_t t = tid >= d ? sh[tid - d] : 0;
+            __syncthreads();
+            sh[tid] += t;
+            __syncthreads();
+        }
+        if (s < nsig) bb[s + 1] = carry + sh[tid];
+        __syncthreads();
+        if (tid == 1023) carry += sh[1023];
+        __syncthreads();
+    }
+}
+
+struct RaggedLayout {
+    Plan pl;
+    int64_t nbmax;
+    WsLayout l;
+    size_t bb, total;
+};
+
+inline RaggedLayout ragged_layout(size_t esz, int64_t nsig, int64_t S, int64_t N) {
+    RaggedLayout r;
+    r.pl = make_plan(esz, 1, 1, N);  // chunk length and batch size depend on the order only
+    const int64_t span = (int64_t)r.pl.G * r.pl.L;
+    r.nbmax = nsig + S / span + 1;
+    r.l = ws_layout(esz, r.nbmax, N);
+    r.bb = r.l.total;
+    r.total = align256(r.bb + (size_t)(nsig + 1) * sizeof(int64_t));
+    return r;
+}
+
+template <typename T>
+ChunkParams<T> ragged_params(const RaggedLayout &r, int64_t nsig, int64_t N, const int64_t *off, void *ws) {
+    ChunkParams<T> p = base_params<T>(r.pl, nsig, 0, N, ws);
+    unsigned char *w = static_cast<unsigned char *>(ws);
+    p.nbatches = r.nbmax;
+    p.roff = off;
+    p.bb = reinterpret_cast<int64_t *>(w + r.bb);
+    p.nsig = nsig;
+    p.as_b = 0;
+    p.as_t = N;
+    return p;
+}
+
+template <typename T>
+cudaError_t ragged_prologue(const RaggedLayout &r, const ChunkParams<T> &p, void *ws, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(ws, 0, r.l.aggP, st);  // header + flags
+    if (e != cudaSuccess) return e;
+    batch_base_kernel<<<1, 1024, 0, st>>>(p.roff, p.nsig, (int64_t)r.pl.G * r.pl.L, p.bb, p.status);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t chunked_ragged_workspace(size_t esz, int64_t nsig, int64_t S, int64_t N) {
+    if (!chunked_supported(N)) return 0;
+    return ragged_layout(esz, nsig, S, N).total;
+}
+
+template <typename T>
+cudaError_t chunked_forward_ragged(const T *x, const T *A, const int64_t *off, const T *zi, T *y, int64_t nsig,
+                                   int64_t S, int64_t N, void *ws, size_t ws_bytes, cudaStream_t st) {
+    const RaggedLayout r = ragged_layout(sizeof(T), nsig, S, N);
+    if (ws_bytes < r.total) return cudaErrorInvalidValue;
+    ChunkParams<T> p = ragged_params<T>(r, nsig, N, off, ws);
+    p.in = x;
+    p.A = A;
+    p.zi = zi;
+    p.out = y;
+    cudaError_t e = ragged_prologue<T>(r, p, ws, st);
+    if (e != cudaSuccess) return e;
+    return dispatch<T, false, false>(p, r.pl.NP, st);
+}
+
+template <typename T>
+cudaError_t chunked_backward_ragged(const T *gy, const T *A, const int64_t *off, const T *zi, const T *y, T *gx,
+                                    T *gA, T *gzi, int64_t nsig, int64_t S, int64_t N, void *ws, size_t ws_bytes,
+                                    cudaStream_t st) {
+    const RaggedLayout r = ragged_layout(sizeof(T), nsig, S, N);
+    if (ws_bytes < r.total) return cudaErrorInvalidValue;
+    ChunkParams<T> p = ragged_params<T>(r, nsig, N, off, ws);
+    p.in = gy;
+    p.A = A;
+    p.zi = zi;
+    p.ysave = y;
+    p.out = gx;
+    p.gA = gA;
+    p.gzi = gzi;
+    cudaError_t e = ragged_prologue<T>(r, p, ws, st);
+    if (e != cudaSuccess) return e;
+    if (gzi) {  // empty signals get no batch: their grad_zi is zero
+        e = cudaMemsetAsync(gzi, 0, (size_t)nsig * N * sizeof(T), st);
+        if (e != cudaSuccess) return e;
+    }
+    return dispatch<T, true, false>(p, r.pl.NP, st);
+}
+
+template cudaError_t chunked_forward_ragged<float>(const float *, const float *, const int64_t *, const float *,
+                                                   float *, int64_t, int64_t, int64_t, void *, size_t, cudaStream_t);
+template cudaError_t chunked_forward_ragged<double>(const double *, const double *, const int64_t *, const double *,
+                                                    double *, int64_t, int64_t, int64_t, void *, size_t, cudaStream_t);
+template cudaError_t chunked_backward_ragged<float>(const float *, const float *, const int64_t *, const float *,
+                                                    const float *, float *, float *, float *, int64_t, int64_t,
+                                                    int64_t, void *, size_t, cudaStream_t);
+template cudaError_t chunked_backward_ragged<double>(const double *, const double *, const int64_t *,
+                                                     const double *, const double *, double *, double *, double *,
+                                                     int64_t, int64_t, int64_t, void *, size_t, cudaStream_t);
 
 template cudaError_t chunked_forward<float>(const FwdArgs<float> &, bool, void *, size_t, cudaStream_t);
 template cudaError_t chunked_forward<double>(const FwdArgs<double> &, bool, void *, size_t, cudaStream_t);

@@ -14,6 +14,16 @@ bool chunked_preferred(int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
 size_t chunked_forward_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
 size_t chunked_backward_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
 
+// Ragged batches (signals concatenated along time, int64 offsets on the device).
+size_t chunked_ragged_workspace(size_t esz, int64_t nsig, int64_t S, int64_t N);
+template <typename T>
+cudaError_t chunked_forward_ragged(const T *x, const T *A, const int64_t *off, const T *zi, T *y, int64_t nsig,
+                                   int64_t S, int64_t N, void *ws, size_t ws_bytes, cudaStream_t st);
+template <typename T>
+cudaError_t chunked_backward_ragged(const T *gy, const T *A, const int64_t *off, const T *zi, const T *y, T *gx,
+                                    T *gA, T *gzi, int64_t nsig, int64_t S, int64_t N, void *ws, size_t ws_bytes,
+                                    cudaStream_t st);
+
 template <typename T>
 cudaError_t chunked_forward(const FwdArgs<T> &p, bool neg, void *ws, size_t ws_bytes,
                             cudaStream_t st);

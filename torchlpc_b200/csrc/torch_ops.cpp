@@ -208,6 +208,81 @@ std::tuple<at::Tensor, at::Tensor, at::Tensor> scan_backward(
     return {gi, gd, g0};
 }
 
+// Ragged batches: x (S,), A (S, N), offsets (nsig+1,) int64 on the same
+// device, zi (nsig, N) or none.
+void check_ragged(const at::Tensor &x, const at::Tensor &A, const at::Tensor &offsets) {
+    TORCH_CHECK(x.dim() == 1, "ragged input must be 1D (S,)");
+    TORCH_CHECK(A.dim() == 2 && A.size(0) == x.size(0), "ragged coefficients must be (S, order)");
+    TORCH_CHECK(A.scalar_type() == x.scalar_type(), "Coefficients must have the same scalar type as input");
+    TORCH_CHECK(offsets.dim() == 1 && offsets.size(0) >= 1 && offsets.scalar_type() == at::kLong,
+                "offsets must be a 1D int64 tensor of nsig+1 sample offsets");
+    check_cuda(x, "x");
+    check_cuda(A, "A");
+    check_cuda(offsets, "offsets");
+    TORCH_CHECK(offsets.device() == x.device(), "offsets must be on the device of x");
+}
+
+at::Tensor lpc_ragged(const at::Tensor &x, const at::Tensor &A, const at::Tensor &offsets,
+                      const c10::optional<at::Tensor> &zi_opt) {
+    check_ragged(x, A, offsets);
+    const int64_t S = x.size(0), N = A.size(1), nsig = offsets.size(0) - 1;
+    at::Tensor zi;
+    if (zi_opt.has_value() && zi_opt->defined()) {
+        zi = zi_opt->contiguous();
+        TORCH_CHECK(zi.scalar_type() == x.scalar_type() && zi.dim() == 2 && zi.size(0) == nsig &&
+                        zi.size(1) == N,
+                    "Initial conditions must be (nsig, order) of the input's dtype");
+    }
+    const int dt = dtype_code(x);
+    const c10::cuda::CUDAGuard guard(x.device());
+    at::Tensor xc = x.contiguous(), ac = A.contiguous(), oc = offsets.contiguous();
+    at::Tensor y = at::empty({S}, x.options());
+    const size_t wsb = lpc_b200_ragged_workspace_size(dt, nsig, S, N);
+    at::Tensor ws = workspace(wsb, x);
+    check_status(lpc_b200_forward_ragged(dt, xc.data_ptr(), ac.data_ptr(), oc.data_ptr<int64_t>(),
+                                         ptr_or_null(zi), y.data_ptr(), nsig, S, N, ptr_or_null(ws), wsb,
+                                         c10::cuda::getCurrentCUDAStream().stream()),
+                 "lpc_ragged");
+    return y;
+}
+
+std::tuple<at::Tensor, at::Tensor, at::Tensor> lpc_backward_ragged(
+    const at::Tensor &grad_y, const at::Tensor &A, const at::Tensor &offsets,
+    const c10::optional<at::Tensor> &zi_opt, const at::Tensor &y, bool need_A, bool need_zi) {
+    check_ragged(y, A, offsets);
+    TORCH_CHECK(grad_y.sizes() == y.sizes() && grad_y.scalar_type() == y.scalar_type(),
+                "grad_y and y must both be (S,) of one dtype");
+    check_cuda(grad_y, "grad_y");
+    const int64_t S = y.size(0), N = A.size(1), nsig = offsets.size(0) - 1;
+    at::Tensor zi;
+    if (zi_opt.has_value() && zi_opt->defined()) {
+        zi = zi_opt->contiguous();
+        TORCH_CHECK(zi.dim() == 2 && zi.size(0) == nsig && zi.size(1) == N, "zi must be (nsig, order)");
+    }
+    const int dt = dtype_code(y);
+    const c10::cuda::CUDAGuard guard(y.device());
+    at::Tensor gyc = grad_y.contiguous(), ac = A.contiguous(), oc = offsets.contiguous(), yc = y.contiguous();
+    at::Tensor gx = at::empty({S}, y.options());
+    at::Tensor gA = need_A ? at::empty({S, N}, y.options()) : at::Tensor();
+    at::Tensor gzi = need_zi ? at::empty({nsig, N}, y.options()) : at::Tensor();
+    const size_t wsb = lpc_b200_ragged_workspace_size(dt, nsig, S, N);
+    at::Tensor ws = workspace(wsb, y);
+    check_status(lpc_b200_backward_ragged(dt, gyc.data_ptr(), ac.data_ptr(), oc.data_ptr<int64_t>(),
+                                          ptr_or_null(zi), yc.data_ptr(), gx.data_ptr(), ptr_or_null(gA),
+                                          ptr_or_null(gzi), nsig, S, N, ptr_or_null(ws), wsb,
+                                          c10::cuda::getCurrentCUDAStream().stream()),
+                 "lpc_backward_ragged");
+    if (!need_A) gA = at::empty({0}, y.options());
+    if (!need_zi) gzi = at::empty({0}, y.options());
+    return {gx, gA, gzi};
+}
+
+at::Tensor cpu_refused_ragged(const at::Tensor &, const at::Tensor &, const at::Tensor &,
+                              const c10::optional<at::Tensor> &) {
+    TORCH_CHECK(false, "torchlpc_b200 runs on CUDA devices only (no CPU implementation)");
+    return at::Tensor();
+}
+
 at::Tensor cpu_refused(const at::Tensor &, const at::Tensor &, const c10::optional<at::Tensor> &, int64_t) {
     TORCH_CHECK(false, "torchlpc_b200 runs on CUDA devices only (no CPU implementation)");
     return at::Tensor();
@@ -219,6 +294,9 @@ TORCH_LIBRARY(torchlpc_b200, m) {
     m.def("lpc(Tensor x, Tensor A, Tensor? zi, int algo=0) -> Tensor");
     m.def("lpc_backward(Tensor grad_y, Tensor A, Tensor? zi, Tensor y, bool need_A, bool need_zi, "
           "int algo=0) -> (Tensor, Tensor, Tensor)");
+    m.def("lpc_ragged(Tensor x, Tensor A, Tensor offsets, Tensor? zi) -> Tensor");
+    m.def("lpc_backward_ragged(Tensor grad_y, Tensor A, Tensor offsets, Tensor? zi, Tensor y, bool need_A, "
+          "bool need_zi) -> (Tensor, Tensor, Tensor)");
     m.def("scan(Tensor input, Tensor weights, Tensor? initials, int algo=0) -> Tensor");
     m.def("scan_backward(Tensor grad_out, Tensor decay, Tensor? init, Tensor out, bool need_decay, "
           "bool need_init, int algo=0) -> (Tensor, Tensor, Tensor)");
@@ -229,9 +307,12 @@ TORCH_LIBRARY_IMPL(torchlpc_b200, CUDA, m) {
     m.impl("lpc_backward", &lpc_backward);
     m.impl("scan", &scan);
     m.impl("scan_backward", &scan_backward);
+    m.impl("lpc_ragged", &lpc_ragged);
+    m.impl("lpc_backward_ragged", &lpc_backward_ragged);
 }
 
 TORCH_LIBRARY_IMPL(torchlpc_b200, CPU, m) {
     m.impl("lpc", &cpu_refused);
     m.impl("scan", &cpu_refused);
+    m.impl("lpc_ragged", &cpu_refused_ragged);
 }
