@@ -24,7 +24,7 @@ def _ragged_case(lengths, N, seed, dtype):
     off[1:] = np.cumsum(lengths)
     S = int(off[-1])
     x = g.standard_normal(S)
-    # stable per-sample filters: poles of radius <= 0.95 with slowly drifting angles
+    # stable per-sample filters: poles of radius <= 0.9 with slowly drifting angles
     A = np.zeros((S, N))
     for s in range(len(lengths)):
         a, b = off[s], off[s + 1]
@@ -32,7 +32,7 @@ def _ragged_case(lengths, N, seed, dtype):
             continue
         t = np.arange(b - a)[:, None]
         P = N // 2
-        r = 0.6 + 0.35 * g.random(P)
+        r = 0.5 + 0.4 * g.random(P)
         th = (np.arange(P) + g.random(P)) * np.pi / max(P, 1)
         th = th[None, :] + 0.2 * np.sin(2 * np.pi * t / 997.0)
         coef = np.zeros((b - a, N + 1))

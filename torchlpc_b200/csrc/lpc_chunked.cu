@@ -1292,6 +1292,12 @@ template <typename T>
 ChunkParams<T> ragged_params(const RaggedLayout &r, int64_t nsig, int64_t N, const int64_t *off, void *ws) {
     ChunkParams<T> p = base_params<T>(r.pl, nsig, 0, N, ws);
     unsigned char *w = static_cast<unsigned char *>(ws);
+    // the batch records are laid out for the worst-case batch count, not the
+    // one-batch plan base_params was given
+    p.flags = reinterpret_cast<unsigned *>(w + r.l.flags);
+    p.aggP = reinterpret_cast<T *>(w + r.l.aggP);
+    p.aggz = reinterpret_cast<double *>(w + r.l.aggz);
+    p.incl = reinterpret_cast<double *>(w + r.l.incl);
     p.nbatches = r.nbmax;
     p.roff = off;
     p.bb = reinterpret_cast<int64_t *>(w + r.bb);
