@@ -43,10 +43,12 @@ enum lpc_dtype { LPC_F32 = 0, LPC_F64 = 1 };
 
 /* Algorithm selection for the forward/backward passes. */
 enum lpc_algo {
-    LPC_ALGO_AUTO = 0,    /* choose by (B, T, N) and the device's SM count          */
+    LPC_ALGO_AUTO = 0,    /* choose by (B, T, N) and the coefficient stride         */
     LPC_ALGO_PLAIN = 1,   /* one warp per signal, sequential in time               */
-    LPC_ALGO_CHUNKED = 2  /* chunked linear-recurrence scan, parallel in time      */
+    LPC_ALGO_CHUNKED = 2, /* chunked linear-recurrence scan, parallel in time      */
                           /* (orders above 32 run the plain kernels)             */
+    LPC_ALGO_TI = 3       /* time-invariant chunked scan (a_stride_t == 0 only;   */
+                          /* otherwise as LPC_ALGO_AUTO)                         */
 };
 
 /* Human-readable text for a status code (static storage). */

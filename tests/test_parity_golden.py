@@ -15,7 +15,7 @@ from tests.gpu_helpers import TOL32, TOL64, err, oracle_fwd_bwd, run_fwd_bwd, to
 
 pytestmark = pytest.mark.gpu
 
-ALGOS = ["plain", "chunked"]
+ALGOS = ["plain", "chunked", "ti"]  # "ti" serves time-invariant cases, the rest as "auto"
 CASES = [n for n in golden_names() if not n.startswith("scan") and "ragged" not in n]
 
 

@@ -9,7 +9,7 @@ import os
 
 import torch
 
-ALGOS = {"auto": 0, "plain": 1, "chunked": 2}
+ALGOS = {"auto": 0, "plain": 1, "chunked": 2, "ti": 3}
 
 try:
     from . import _C  # noqa: F401  (registers torch.ops.torchlpc_b200.*)
@@ -24,7 +24,8 @@ _algo = ALGOS[os.environ.get("LPC_B200_ALGO", "auto")]
 
 
 def set_algo(name: str) -> None:
-    """Select the kernel family: "auto" (default), "plain" or "chunked"."""
+    """Select the kernel family: "auto" (default), "plain", "chunked" or "ti"
+    (time-invariant coefficients only; other calls fall back as "auto")."""
     global _algo
     _algo = ALGOS[name]
 
@@ -35,7 +36,7 @@ def get_algo() -> str:
 
 def available_algos():
     """Kernel families this build can run ("auto" picks among them)."""
-    return ["plain", "chunked"] if _CHUNKED else ["plain"]
+    return ["plain", "chunked", "ti"] if _CHUNKED else ["plain"]
 
 
 _CHUNKED = True

@@ -33,8 +33,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                      "--expt-relaxed-constexpr", f"-I{INCLUDE}"]
 
-CU_SOURCES = ["lpc_plain.cu", "lpc_chunked.cu", "lpc_capi.cu", "lpc_noalloc.cu"]
-HEADERS = ["lpc_common.cuh", "lpc_plain.cuh", "lpc_chunked.cuh"]
+CU_SOURCES = ["lpc_plain.cu", "lpc_chunked.cu", "lpc_ti.cu", "lpc_capi.cu", "lpc_noalloc.cu"]
+HEADERS = ["lpc_common.cuh", "lpc_plain.cuh", "lpc_chunked.cuh", "lpc_ti.cuh"]
 
 
 def _newer(target: Path, deps) -> bool:

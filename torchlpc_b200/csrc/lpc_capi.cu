@@ -6,6 +6,7 @@
 
 #include "lpc_chunked.cuh"
 #include "lpc_plain.cuh"
+#include "lpc_ti.cuh"
 
 using namespace lpcb;
 
@@ -19,13 +20,22 @@ bool sizes_ok(int64_t B, int64_t T, int64_t N) {
     return B >= 0 && T >= 0 && N >= 1 && N <= kMaxOrder && B < (int64_t(1) << 31);
 }
 
-// Choice between the sequential and the chunked kernels.
+// Choice between the sequential, the chunked and the time-invariant kernels.
 // LPC_ALGO_CHUNKED falls back to the plain kernels for orders the chunked
-// kernels do not cover (N > 32).
+// kernels do not cover (N > 32); LPC_ALGO_TI applies to a_stride_t == 0 only.
+// AUTO: time-invariant coefficients with at least 2048 samples per signal take
+// the time-invariant scan, long time-varying signals the chunked scan.
 int resolve_algo(int algo, int64_t B, int64_t T, int64_t N, int64_t a_stride_t) {
     if (algo == LPC_ALGO_PLAIN) return algo;
     if (algo == LPC_ALGO_CHUNKED) return chunked_supported(N) ? algo : LPC_ALGO_PLAIN;
+    if (a_stride_t == 0 && ti_supported(N) && (algo == LPC_ALGO_TI || T >= 2048)) return LPC_ALGO_TI;
     return chunked_preferred(B, T, N, a_stride_t) ? LPC_ALGO_CHUNKED : LPC_ALGO_PLAIN;
+}
+
+size_t workspace_for(int algo, size_t esz, int64_t B, int64_t T, int64_t N, int64_t a_stride_t) {
+    if (algo == LPC_ALGO_CHUNKED) return chunked_forward_workspace(esz, B, T, N, a_stride_t);
+    if (algo == LPC_ALGO_TI) return ti_workspace(esz, B, T, N);
+    return 0;
 }
 
 template <typename T>
@@ -38,6 +48,10 @@ int forward_t(int algo, const void *x, const void *A, const void *zi, void *y, i
     if (algo == LPC_ALGO_CHUNKED) {
         if (ws_bytes < chunked_forward_workspace(sizeof(T), B, T_, N, st)) return LPC_ERR_WORKSPACE;
         return cuda_status(chunked_forward<T>(p, false, ws, ws_bytes, stream));
+    }
+    if (algo == LPC_ALGO_TI) {
+        if (!ws || ws_bytes < ti_workspace(sizeof(T), B, T_, N)) return LPC_ERR_WORKSPACE;
+        return cuda_status(ti_forward<T>(p, ws, ws_bytes, stream));
     }
     return cuda_status(plain_forward<T>(p, false, stream));
 }
@@ -58,6 +72,10 @@ int backward_t(int algo, const void *gy, const void *A, const void *zi, const vo
     if (algo == LPC_ALGO_CHUNKED) {
         if (ws_bytes < chunked_backward_workspace(sizeof(T), B, T_, N, st)) return LPC_ERR_WORKSPACE;
         return cuda_status(chunked_backward<T>(p, false, ws, ws_bytes, stream));
+    }
+    if (algo == LPC_ALGO_TI) {
+        if (!ws || ws_bytes < ti_workspace(sizeof(T), B, T_, N)) return LPC_ERR_WORKSPACE;
+        return cuda_status(ti_backward<T>(p, ws, ws_bytes, stream));
     }
     return cuda_status(plain_backward<T>(p, false, stream));
 }
@@ -83,8 +101,7 @@ int lpc_b200_version(void) { return 100; }
 size_t lpc_b200_forward_workspace_size(int dtype, int algo, int64_t B, int64_t T, int64_t N,
                                        int64_t a_stride_t) {
     if (!dtype_ok(dtype) || !sizes_ok(B, T, N)) return 0;
-    if (resolve_algo(algo, B, T, N, a_stride_t) != LPC_ALGO_CHUNKED) return 0;
-    return chunked_forward_workspace(dtype == LPC_F32 ? 4 : 8, B, T, N, a_stride_t);
+    return workspace_for(resolve_algo(algo, B, T, N, a_stride_t), dtype == LPC_F32 ? 4 : 8, B, T, N, a_stride_t);
 }
 
 int lpc_b200_forward(int dtype, int algo, const void *x, const void *A, const void *zi, void *y,
@@ -106,8 +123,7 @@ int lpc_b200_forward(int dtype, int algo, const void *x, const void *A, const vo
 size_t lpc_b200_backward_workspace_size(int dtype, int algo, int64_t B, int64_t T, int64_t N,
                                         int64_t a_stride_t) {
     if (!dtype_ok(dtype) || !sizes_ok(B, T, N)) return 0;
-    if (resolve_algo(algo, B, T, N, a_stride_t) != LPC_ALGO_CHUNKED) return 0;
-    return chunked_backward_workspace(dtype == LPC_F32 ? 4 : 8, B, T, N, a_stride_t);
+    return workspace_for(resolve_algo(algo, B, T, N, a_stride_t), dtype == LPC_F32 ? 4 : 8, B, T, N, a_stride_t);
 }
 
 int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A, const void *zi,

@@ -39,6 +39,7 @@
 // kernel over the grad_x just written); grad_zi is the adjoint carried N steps
 // past t = 0.
 #include "lpc_chunked.cuh"
+#include "lpc_ti.cuh"
 
 namespace lpcb {
 
@@ -990,74 +991,6 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
 }
 
 // ----------------------------------------------------------------------------
-// Time-invariant coefficients: grad_a[b,i] = sgn * sum_t grad_x[b,t] *
-// ypad[b,t-1-i] with ypad(-1-k) = zi[b,k] (zero past k = N-1), from the
-// grad_x the chunked backward has written.  Block (x, b) reduces a strided
-// share of signal b and adds its per-tap sums atomically.
-// ----------------------------------------------------------------------------
-template <typename T, int NP>
-__global__ void __launch_bounds__(256) ti_grad_kernel(const T *gx, const T *y, const T *zi, T *ga, int64_t B,
-                                                     int64_t T_, int N, T sgn) {
-    __shared__ T part[8][NP];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
-        const T *gb = gx + b * T_;
-        const T *yb = y + b * T_;
-        const T *zb = zi ? zi + b * N : nullptr;
-        T acc[NP];
-#pragma unroll
-        for (int i = 0; i < NP; ++i) acc[i] = T(0);
-        for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T_;
-             t += (int64_t)gridDim.x * blockDim.x) {
-            const T g = gb[t];
-#pragma unroll
-            for (int i = 0; i < NP; ++i) {
-                if (i < N) {
-                    const int64_t j = t - 1 - i;
-                    const T yy = j >= 0 ? yb[j] : ((zb && i - t < N) ? zb[i - t] : T(0));
-                    acc[i] = fma(g, yy, acc[i]);
-                }
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < NP; ++i) {
-            T v = acc[i];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) part[warp][i] = v;
-        }
-        __syncthreads();
-        if (threadIdx.x < N && threadIdx.x < NP) {
-            T v = T(0);
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += part[w][threadIdx.x];
-            if (v != T(0)) atomicAdd(ga + b * N + threadIdx.x, sgn * v);
-        }
-        __syncthreads();
-    }
-}
-
-template <typename T, int NP>
-cudaError_t launch_ti_grad(const T *gx, const T *y, const T *zi, T *ga, int64_t B, int64_t T_, int N, bool neg,
-                           cudaStream_t st) {
-    const int64_t per_block = 256 * 64;  // samples a block covers per signal
-    const unsigned gxd = (unsigned)min64(4096, (T_ + per_block - 1) / per_block);
-    const unsigned gyd = (unsigned)min64(65535, B);
-    ti_grad_kernel<T, NP><<<dim3(gxd, gyd), 256, 0, st>>>(gx, y, zi, ga, B, T_, N, neg ? T(1) : T(-1));
-    return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t ti_grad(const BwdArgs<T> &a, bool neg, int NP, cudaStream_t st) {
-    switch (NP) {
-#define LPCB_CASE(n) \
-    case n: return launch_ti_grad<T, n>(a.gx, a.y, a.zi, a.gA, a.B, a.T, (int)a.N, neg, st);
-        LPCB_FOR_EACH_NP(LPCB_CASE)
-#undef LPCB_CASE
-        default: return cudaErrorNotSupported;
-    }
-}
-
-// ----------------------------------------------------------------------------
 // Host side.
 // ----------------------------------------------------------------------------
 constexpr int kChunkLen = 256;   // target chunk length; rounded to an even number of windows
@@ -1204,10 +1137,6 @@ cudaError_t chunked_backward(const BwdArgs<T> &a, bool neg, void *ws, size_t ws_
     if (ws_bytes < l.total) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(ws, 0, l.aggP, st);
     if (e != cudaSuccess) return e;
-    if (a.gA && a.a_stride_t == 0) {
-        e = cudaMemsetAsync(a.gA, 0, (size_t)a.B * a.N * sizeof(T), st);
-        if (e != cudaSuccess) return e;
-    }
     ChunkParams<T> p = base_params<T>(pl, a.B, a.T, a.N, ws);
     p.in = a.gy;
     p.A = a.A;
@@ -1220,7 +1149,7 @@ cudaError_t chunked_backward(const BwdArgs<T> &a, bool neg, void *ws, size_t ws_
     p.gzi = a.gzi;
     e = neg ? dispatch<T, true, true>(p, pl.NP, st) : dispatch<T, true, false>(p, pl.NP, st);
     if (e != cudaSuccess || !a.gA || a.a_stride_t != 0) return e;
-    return ti_grad<T>(a, neg, pl.NP, st);  // reads the grad_x just written
+    return ti_grad_a<T>(a.gx, a.y, a.zi, a.gA, a.B, a.T, a.N, neg, st);  // reads the grad_x just written
 }
 
 // ----------------------------------------------------------------------------

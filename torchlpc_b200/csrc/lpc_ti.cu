@@ -1,0 +1,371 @@
+// Time-invariant all-pole filter (one coefficient set per signal), parallel in
+// time.  The time-varying chunked scan pays N basis filters per sample to
+// learn each chunk's transition; with constant coefficients every chunk of a
+// signal has the same transition P = C^L (C the companion matrix), so:
+//
+//  1. power    one CTA per signal: P = C^L by square-and-multiply in FP64.
+//  2. zero     one thread per (signal, chunk): the chunk filtered from zero
+//              state; its exit state z_c is stored.
+//  3. combine  one warp per signal: entry states s_{c+1} = P s_c + z_c in
+//              FP64, lane r holding row r of P.
+//  4. fix      one thread per (signal, chunk): the chunk filtered again from
+//              its exact entry state; outputs written.
+//
+// The backward is the same filter over reversed time on grad_y (for constant
+// coefficients the adjoint's coefficient diagonal A[t+1+i, i] is just a[i]),
+// followed by the per-tap reduction grad_a[i] = -sum_t grad_x[t] y[t-1-i] and
+// grad_zi[k] = -sum_{i>=k} a[i] grad_x[i-k] (torchlpc/core.py:186-229 with a
+// stride-0 A).  Coefficients and history live in registers; the history is a
+// ring indexed by compile-time positions (steps unrolled by the padded order).
+#include "lpc_ti.cuh"
+
+namespace lpcb {
+
+namespace {
+
+constexpr int kTiChunk = 1024;  // target chunk length, rounded to a multiple of the padded order
+
+inline int ti_chunk_len(int NP) { return NP * ((kTiChunk + NP - 1) / NP); }
+inline size_t al256(size_t v) { return (v + 255) & ~size_t(255); }
+
+struct TiLayout {
+    int NP, Lc;
+    int64_t nc;
+    size_t P, zst, est, total;
+};
+
+inline TiLayout ti_layout(size_t esz, int64_t B, int64_t T, int64_t N) {
+    TiLayout l;
+    l.NP = padded_order(N);
+    l.Lc = ti_chunk_len(l.NP);
+    l.nc = (T + l.Lc - 1) / l.Lc;
+    size_t off = 0;
+    l.P = off;  // [B][NP][NP] FP64 chunk transitions
+    off = al256(off + (size_t)B * l.NP * l.NP * sizeof(double));
+    l.zst = off;  // [B][nc][NP] zero-state exit states
+    off = al256(off + (size_t)B * l.nc * l.NP * esz);
+    l.est = off;  // [B][nc][NP] exact entry states
+    off = al256(off + (size_t)B * l.nc * l.NP * esz);
+    l.total = off;
+    return l;
+}
+
+template <typename F>
+struct TiArgs {
+    const F *in;   // forward x, backward grad_y: (B,T)
+    const F *a;    // a[b,i] = a[b*as_b + i]
+    const F *zi;   // forward initial state (B,N) or nullptr
+    F *out;        // forward y, backward grad_x
+    int64_t as_b, B, T, nc;
+    int N, Lc;
+    double *P;
+    F *zst, *est;
+};
+
+// acc - sum_i a[i] * h[(u-1-i) mod NP]: four partial chains over the older
+// taps, the newest tap last (one FMA on the loop-carried path).
+template <typename T, int NP>
+__device__ __forceinline__ T ti_step(const T (&a)[NP], const T (&h)[NP], int u, T acc) {
+    if constexpr (NP == 1) {
+        return fma(-a[0], h[0], acc);
+    } else {
+        T q[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+        for (int i = 1; i < NP; ++i) q[i & 3] = fma(a[i], h[(u - 1 - i + 2 * NP) % NP], q[i & 3]);
+        acc = acc - ((q[0] + q[1]) + (q[2] + q[3]));
+        return fma(-a[0], h[(u - 1 + NP) % NP], acc);
+    }
+}
+
+// State vector of the direct form: s[i] = y[t0-1-i] sits at ring slot NP-1-i
+// at a block boundary.
+template <int NP>
+__device__ __forceinline__ constexpr int ti_slot(int i) {
+    return NP - 1 - i;
+}
+
+// ---------------------------------------------------------------- power
+// P = C^Lc, C the companion matrix of the padded order: row 0 is -a, row j
+// (j >= 1) is the unit vector e_{j-1}.  Square-and-multiply in shared memory.
+template <typename T, int NP>
+__global__ void __launch_bounds__(256) ti_power_kernel(const T *a, int64_t as_b, int N, int Lc, double *P) {
+    __shared__ double M[NP][NP + 1], R[NP][NP + 1], W[NP][NP + 1];
+    const int64_t b = blockIdx.x;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < NP * NP; e += blockDim.x) {
+        const int r = e / NP, c = e - (e / NP) * NP;
+        double m = 0.0;
+        if (r == 0)
+            m = c < N ? -(double)a[b * as_b + c] : 0.0;
+        else
+            m = (c == r - 1) ? 1.0 : 0.0;
+        M[r][c] = m;
+        R[r][c] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    // W <- X * Y, then X <- W (X, Y in shared memory; X may equal Y)
+    auto mul_into = [&](double (*X)[NP + 1], double (*Y)[NP + 1]) {
+        for (int e = tid; e < NP * NP; e += blockDim.x) {
+            const int r = e / NP, c = e - (e / NP) * NP;
+            double v = 0.0;
+#pragma unroll 8
+            for (int k = 0; k < NP; ++k) v = fma(X[r][k], Y[k][c], v);
+            W[r][c] = v;
+        }
+        __syncthreads();
+        for (int e = tid; e < NP * NP; e += blockDim.x) {
+            const int r = e / NP, c = e - (e / NP) * NP;
+            X[r][c] = W[r][c];
+        }
+        __syncthreads();
+    };
+    for (int e = Lc; e > 0; e >>= 1) {
+        if (e & 1) mul_into(R, M);
+        if (e > 1) mul_into(M, M);
+    }
+    for (int e = tid; e < NP * NP; e += blockDim.x) P[(size_t)b * NP * NP + e] = R[e / NP][e % NP];
+}
+
+// ---------------------------------------------------------------- zero / fix
+// FIX = false: chunk from zero state, exit state to zst.  FIX = true: chunk
+// from its entry state est, outputs written.  REV: time runs backwards
+// (index T-1-s of in/out for step s).
+template <typename T, int NP, bool REV, bool FIX>
+__global__ void __launch_bounds__(256) ti_chunk_kernel(TiArgs<T> p) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= p.B * p.nc) return;
+    const int64_t b = idx / p.nc;
+    const int64_t c = idx - b * p.nc;
+    const int N = p.N;
+    T a[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) a[i] = i < N ? p.a[b * p.as_b + i] : T(0);
+    T h[NP];
+    if constexpr (FIX) {
+        const T *e = p.est + (size_t)idx * NP;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) h[ti_slot<NP>(i)] = e[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) h[i] = T(0);
+    }
+    const T *inb = p.in + b * p.T;
+    T *outb = p.out + b * p.T;
+    const int64_t s0 = c * p.Lc;
+    const int nblk = (int)((min64(p.Lc, p.T - s0) + NP - 1) / NP);  // blocks holding samples
+#pragma unroll 1
+    for (int blk = 0; blk < nblk; ++blk) {
+        const int64_t sb = s0 + (int64_t)blk * NP;
+#pragma unroll
+        for (int u = 0; u < NP; ++u) {
+            const int64_t s = sb + u;
+            const bool in_range = s < p.T;
+            const int64_t t = REV ? p.T - 1 - s : s;
+            const T xv = in_range ? inb[t] : T(0);
+            h[u] = ti_step<T, NP>(a, h, u, xv);
+            if (FIX && in_range) outb[t] = h[u];
+        }
+    }
+    if constexpr (!FIX) {
+        // exit state after the chunk's blocks (a partial last chunk has no successor)
+        T *z = p.zst + (size_t)idx * NP;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) z[i] = h[ti_slot<NP>(i)];
+    }
+}
+
+// ---------------------------------------------------------------- combine
+// One warp per signal: lane r keeps row r of P; s_{c+1} = P s_c + z_c (FP64).
+template <typename T, int NP, bool REV>
+__global__ void __launch_bounds__(256) ti_combine_kernel(TiArgs<T> p) {
+    const int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (b >= p.B) return;  // whole warps: b is uniform across a warp
+    const bool row = lane < NP;
+    double Pr[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) Pr[q] = row ? p.P[((size_t)b * NP + lane) * NP + q] : 0.0;
+    double s = 0.0;
+    if (!REV && row && p.zi && lane < p.N) s = (double)p.zi[b * p.N + lane];
+    for (int64_t c = 0; c < p.nc; ++c) {
+        const size_t base = ((size_t)b * p.nc + c) * NP;
+        if (row) p.est[base + lane] = (T)s;
+        if (c + 1 == p.nc) break;
+        double v = row ? (double)p.zst[base + lane] : 0.0;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) v = fma(Pr[q], __shfl_sync(0xffffffffu, s, q), v);
+        s = v;
+    }
+}
+
+// ---------------------------------------------------------------- gradients
+// grad_a[b,i] = sgn * sum_t grad_x[b,t] * ypad[b,t-1-i], ypad(-1-k) = zi[b,k].
+template <typename T, int NP>
+__global__ void __launch_bounds__(256) ti_grad_a_kernel(const T *gx, const T *y, const T *zi, T *ga, int64_t B,
+                                                       int64_t T_, int N, T sgn) {
+    __shared__ T part[8][NP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
+        const T *gb = gx + b * T_;
+        const T *yb = y + b * T_;
+        const T *zb = zi ? zi + b * N : nullptr;
+        T acc[NP];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) acc[i] = T(0);
+        for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T_;
+             t += (int64_t)gridDim.x * blockDim.x) {
+            const T g = gb[t];
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                if (i < N) {
+                    const int64_t j = t - 1 - i;
+                    const T yy = j >= 0 ? yb[j] : ((zb && i - t < N) ? zb[i - t] : T(0));
+                    acc[i] = fma(g, yy, acc[i]);
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+            T v = acc[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) part[warp][i] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < N && threadIdx.x < NP) {
+            T v = T(0);
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += part[w][threadIdx.x];
+            if (v != T(0)) atomicAdd(ga + b * N + threadIdx.x, sgn * v);
+        }
+        __syncthreads();
+    }
+}
+
+// grad_zi[b,k] = -sum_{i=k}^{N-1} a[b,i] grad_x[b,i-k]  (grad_x beyond T is 0)
+template <typename T>
+__global__ void ti_grad_zi_kernel(const T *gx, const T *a, int64_t as_b, T *gzi, int64_t B, int64_t T_, int N) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= B * N) return;
+    const int64_t b = e / N;
+    const int k = (int)(e - b * N);
+    T v = T(0);
+    for (int i = k; i < N; ++i)
+        if (i - k < T_) v = fma(-a[b * as_b + i], gx[b * T_ + (i - k)], v);
+    gzi[e] = v;
+}
+
+template <typename T, int NP, bool REV>
+cudaError_t ti_run(TiArgs<T> p, cudaStream_t st) {
+    ti_power_kernel<T, NP><<<(unsigned)p.B, 256, 0, st>>>(p.a, p.as_b, p.N, p.Lc, p.P);
+    const int64_t threads = p.B * p.nc;
+    const unsigned g1 = (unsigned)((threads + 255) / 256);
+    ti_chunk_kernel<T, NP, REV, false><<<g1, 256, 0, st>>>(p);
+    ti_combine_kernel<T, NP, REV><<<(unsigned)((p.B * 32 + 255) / 256), 256, 0, st>>>(p);
+    ti_chunk_kernel<T, NP, REV, true><<<g1, 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+template <typename T, bool REV>
+cudaError_t ti_dispatch(const TiArgs<T> &p, int NP, cudaStream_t st) {
+    switch (NP) {
+#define LPCB_CASE(n) \
+    case n: return ti_run<T, n, REV>(p, st);
+        LPCB_FOR_EACH_NP(LPCB_CASE)
+#undef LPCB_CASE
+        default: return cudaErrorNotSupported;
+    }
+}
+
+template <typename T>
+TiArgs<T> ti_args(const TiLayout &l, const T *in, const T *a, int64_t as_b, const T *zi, T *out, int64_t B,
+                  int64_t T_, int64_t N, void *ws) {
+    unsigned char *w = static_cast<unsigned char *>(ws);
+    TiArgs<T> p{};
+    p.in = in;
+    p.a = a;
+    p.as_b = as_b;
+    p.zi = zi;
+    p.out = out;
+    p.B = B;
+    p.T = T_;
+    p.nc = l.nc;
+    p.N = (int)N;
+    p.Lc = l.Lc;
+    p.P = reinterpret_cast<double *>(w + l.P);
+    p.zst = reinterpret_cast<T *>(w + l.zst);
+    p.est = reinterpret_cast<T *>(w + l.est);
+    return p;
+}
+
+template <typename T, int NP>
+cudaError_t launch_grad_a(const T *gx, const T *y, const T *zi, T *ga, int64_t B, int64_t T_, int N, T sgn,
+                          cudaStream_t st) {
+    const int64_t per_block = 256 * 64;  // samples a block covers per signal
+    const unsigned gxd = (unsigned)min64(4096, (T_ + per_block - 1) / per_block);
+    const unsigned gyd = (unsigned)min64(65535, B);
+    ti_grad_a_kernel<T, NP><<<dim3(gxd, gyd), 256, 0, st>>>(gx, y, zi, ga, B, T_, N, sgn);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool ti_supported(int64_t N) { return N >= 1 && N <= 32; }
+
+size_t ti_workspace(size_t esz, int64_t B, int64_t T, int64_t N) {
+    if (!ti_supported(N)) return 0;
+    return ti_layout(esz, B, T, N).total;
+}
+
+template <typename T>
+cudaError_t ti_grad_a(const T *gx, const T *y, const T *zi, T *ga, int64_t B, int64_t T_, int64_t N, bool neg,
+                      cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(ga, 0, (size_t)B * N * sizeof(T), st);
+    if (e != cudaSuccess) return e;
+    const T sgn = neg ? T(1) : T(-1);
+    switch (padded_order(N)) {
+#define LPCB_CASE(n) \
+    case n: return launch_grad_a<T, n>(gx, y, zi, ga, B, T_, (int)N, sgn, st);
+        LPCB_FOR_EACH_NP(LPCB_CASE)
+#undef LPCB_CASE
+        default: return cudaErrorNotSupported;
+    }
+}
+
+template <typename T>
+cudaError_t ti_forward(const FwdArgs<T> &a, void *ws, size_t ws_bytes, cudaStream_t st) {
+    const TiLayout l = ti_layout(sizeof(T), a.B, a.T, a.N);
+    if (ws_bytes < l.total) return cudaErrorInvalidValue;
+    const TiArgs<T> p = ti_args<T>(l, a.x, a.A, a.a_stride_b, a.zi, a.y, a.B, a.T, a.N, ws);
+    return ti_dispatch<T, false>(p, l.NP, st);
+}
+
+template <typename T>
+cudaError_t ti_backward(const BwdArgs<T> &a, void *ws, size_t ws_bytes, cudaStream_t st) {
+    const TiLayout l = ti_layout(sizeof(T), a.B, a.T, a.N);
+    if (ws_bytes < l.total) return cudaErrorInvalidValue;
+    const TiArgs<T> p = ti_args<T>(l, a.gy, a.A, a.a_stride_b, nullptr, a.gx, a.B, a.T, a.N, ws);
+    cudaError_t e = ti_dispatch<T, true>(p, l.NP, st);
+    if (e != cudaSuccess) return e;
+    if (a.gA) {
+        e = ti_grad_a<T>(a.gx, a.y, a.zi, a.gA, a.B, a.T, a.N, false, st);
+        if (e != cudaSuccess) return e;
+    }
+    if (a.gzi) {
+        const int64_t n = a.B * a.N;
+        ti_grad_zi_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.gx, a.A, a.a_stride_b, a.gzi, a.B, a.T,
+                                                                          (int)a.N);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+template cudaError_t ti_grad_a<float>(const float *, const float *, const float *, float *, int64_t, int64_t,
+                                      int64_t, bool, cudaStream_t);
+template cudaError_t ti_grad_a<double>(const double *, const double *, const double *, double *, int64_t, int64_t,
+                                       int64_t, bool, cudaStream_t);
+template cudaError_t ti_forward<float>(const FwdArgs<float> &, void *, size_t, cudaStream_t);
+template cudaError_t ti_forward<double>(const FwdArgs<double> &, void *, size_t, cudaStream_t);
+template cudaError_t ti_backward<float>(const BwdArgs<float> &, void *, size_t, cudaStream_t);
+template cudaError_t ti_backward<double>(const BwdArgs<double> &, void *, size_t, cudaStream_t);
+
+}  // namespace lpcb
