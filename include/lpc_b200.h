@@ -57,6 +57,14 @@ const char *lpc_b200_status_string(int status);
 /* ABI version of this library (major*10000 + minor*100 + patch). */
 int lpc_b200_version(void);
 
+/* Target chunk length (samples) of the chunked scan, process-wide: the
+ * autotuner's knob (no reference counterpart).  <= 0 restores the default
+ * (256); values are clamped to [32, 4096] and rounded up to an even number of
+ * the kernel's windows.  Workspace sizes follow the current setting, so change
+ * it only between calls. */
+int lpc_b200_set_chunk_length(int64_t samples);
+int64_t lpc_b200_chunk_length(void);
+
 /* ---------------------------------------------------------------------------
  * Forward filter.
  * Replaces the reference operator torchlpc::lpc(x, A, zi) -> y
@@ -110,6 +118,26 @@ int lpc_b200_forward_noalloc(int dtype, const void *x, const void *A,
                              const void *zi, void *y, int64_t B, int64_t T,
                              int64_t N, int64_t a_stride_b, int64_t a_stride_t,
                              void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Failure detection.  No reference counterpart (the reference kernels have no
+ * bounded waits).  The chunked kernels' waits on other CTAs are bounded; when
+ * one gives up it ORs a code into the status word of the call's workspace
+ * (1: a predecessor's flag never appeared, 2: inconsistent flags, 8: a ragged
+ * signal with a negative length) and the launch completes instead of hanging.
+ * lpc_b200_workspace_status reads that word (synchronises `stream`); the
+ * word is cleared by the next chunked call that uses the workspace.
+ * lpc_b200_selftest_timeout runs a chunked forward whose look-back waits for
+ * a flag nothing sets, with the given spin limit (polls of about a
+ * microsecond each), and returns LPC_ERR_TIMEOUT with the recorded word in
+ * *status when the wait gave up as designed.
+ * ------------------------------------------------------------------------- */
+int lpc_b200_workspace_status(const void *workspace, unsigned *status, void *stream);
+
+size_t lpc_b200_selftest_workspace_size(void);
+
+int lpc_b200_selftest_timeout(void *workspace, size_t workspace_bytes,
+                              unsigned spin_limit, unsigned *status, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Ragged batches.  No reference counterpart (the reference operators take a

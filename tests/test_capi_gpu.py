@@ -67,3 +67,33 @@ def test_workspace_too_small_is_reported(lib):
         pytest.skip("chunked path needs no workspace here")
     rc = lib.lpc_b200_forward(0, 2, p(x), p(A), None, p(y), 2, 1 << 16, 16, 16 << 16, 16, None, 0, st)
     assert rc == 3
+
+
+def test_bounded_lookback_wait_reports_timeout_and_context_survives(lib):
+    """A chunked forward whose ticket queue skips batch 0: batch 1 waits for a
+    flag nothing sets.  The wait gives up after its spin limit, the status word
+    carries code 1, the call returns LPC_ERR_TIMEOUT, and the context still runs
+    ordinary work afterwards (no trap, no hang)."""
+    lib.lpc_b200_selftest_workspace_size.restype = sz
+    lib.lpc_b200_selftest_timeout.argtypes = [vp, sz, C.c_uint, C.POINTER(C.c_uint), vp]
+    lib.lpc_b200_workspace_status.argtypes = [vp, C.POINTER(C.c_uint), vp]
+    wsb = lib.lpc_b200_selftest_workspace_size()
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    status = C.c_uint(0)
+    rc = lib.lpc_b200_selftest_timeout(p(ws), wsb, 2000, C.byref(status), st)
+    assert rc == 5, rc
+    assert status.value & 1
+    again = C.c_uint(0)
+    assert lib.lpc_b200_workspace_status(p(ws), C.byref(again), st) == 0 and again.value == status.value
+    # the context is intact: an ordinary call through the same library works
+    w = make_workload("cfg3", seed=1, B=2, T=40000)
+    x, A, zi = (w[k].cuda() for k in ("x", "A", "zi"))
+    B, T, N = A.shape
+    y = torch.empty_like(x)
+    wsb = lib.lpc_b200_forward_workspace_size(0, 2, B, T, N, N)
+    ws2 = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+    assert lib.lpc_b200_forward(0, 2, p(x), p(A), p(zi), p(y), B, T, N, T * N, N, p(ws2), wsb, st) == 0
+    ok = C.c_uint(7)
+    assert lib.lpc_b200_workspace_status(p(ws2), C.byref(ok), st) == 0 and ok.value == 0
+    assert O.normwise_err(y, O.lpc_forward(w["x"], w["A"], w["zi"])) < 1e-4

@@ -20,18 +20,59 @@ except ImportError as e:  # pragma: no cover - exercised only without a build
     EXTENSION_LOADED = False
     _LOAD_ERROR = e
 
-_algo = ALGOS[os.environ.get("LPC_B200_ALGO", "auto")]
+TUNED = -1  # "tuned": per-shape choice from torchlpc_b200.tune
+_algo = TUNED if os.environ.get("LPC_B200_ALGO") == "tuned" else ALGOS[os.environ.get("LPC_B200_ALGO", "auto")]
+_LIB = None
+
+
+def _lib():
+    """The C ABI library the operators are linked against (same instance)."""
+    import ctypes
+    from pathlib import Path
+
+    global _LIB
+    if _LIB is None:
+        lib = ctypes.CDLL(str(Path(__file__).resolve().parent / "liblpc_b200.so"))
+        lib.lpc_b200_set_chunk_length.argtypes = [ctypes.c_int64]
+        lib.lpc_b200_chunk_length.restype = ctypes.c_int64
+        _LIB = lib
+    return _LIB
+
+
+def set_chunk_length(samples: int) -> None:
+    """Target chunk length of the chunked scan (0 restores the default)."""
+    _require()
+    _lib().lpc_b200_set_chunk_length(int(samples))
+
+
+def get_chunk_length() -> int:
+    _require()
+    return int(_lib().lpc_b200_chunk_length())
 
 
 def set_algo(name: str) -> None:
-    """Select the kernel family: "auto" (default), "plain", "chunked" or "ti"
-    (time-invariant coefficients only; other calls fall back as "auto")."""
+    """Select the kernel family: "auto" (default), "plain", "chunked", "ti"
+    (time-invariant coefficients only; other calls fall back as "auto") or
+    "tuned" (the autotuner's choice per shape, tuning unseen shapes on first
+    use)."""
     global _algo
-    _algo = ALGOS[name]
+    _algo = TUNED if name == "tuned" else ALGOS[name]
 
 
 def get_algo() -> str:
-    return {v: k for k, v in ALGOS.items()}[_algo]
+    return "tuned" if _algo == TUNED else {v: k for k, v in ALGOS.items()}[_algo]
+
+
+def _resolve(x, A):
+    """Algorithm code for one call (the tuner's choice in "tuned" mode)."""
+    if _algo != TUNED:
+        return _algo
+    from . import tune
+
+    B, T = x.shape
+    cfg = tune.choice(B, T, A.shape[-1], x.dtype, A.dim() == 2 or A.stride(1) == 0, x.device)
+    set_chunk_length(cfg["chunk"])
+    return ALGOS[cfg["algo"]]
 
 
 def available_algos():
@@ -51,22 +92,22 @@ def _require():
 
 def lpc(x, A, zi):
     _require()
-    return torch.ops.torchlpc_b200.lpc(x, A, zi, _algo)
+    return torch.ops.torchlpc_b200.lpc(x, A, zi, _resolve(x, A))
 
 
 def lpc_backward(grad_y, A, zi, y, need_A, need_zi):
     _require()
-    return torch.ops.torchlpc_b200.lpc_backward(grad_y, A, zi, y, need_A, need_zi, _algo)
+    return torch.ops.torchlpc_b200.lpc_backward(grad_y, A, zi, y, need_A, need_zi, _resolve(y, A))
 
 
 def scan(impulse, decay, init):
     _require()
-    return torch.ops.torchlpc_b200.scan(impulse, decay, init, _algo)
+    return torch.ops.torchlpc_b200.scan(impulse, decay, init, max(_algo, 0))
 
 
 def scan_backward(grad_out, decay, init, out, need_decay, need_init):
     _require()
-    return torch.ops.torchlpc_b200.scan_backward(grad_out, decay, init, out, need_decay, need_init, _algo)
+    return torch.ops.torchlpc_b200.scan_backward(grad_out, decay, init, out, need_decay, need_init, max(_algo, 0))
 
 
 def lpc_ragged(x, A, offsets, zi):

@@ -98,6 +98,13 @@ const char *lpc_b200_status_string(int status) {
 
 int lpc_b200_version(void) { return 100; }
 
+int lpc_b200_set_chunk_length(int64_t samples) {
+    set_chunk_target(samples);
+    return LPC_OK;
+}
+
+int64_t lpc_b200_chunk_length(void) { return chunk_target(); }
+
 size_t lpc_b200_forward_workspace_size(int dtype, int algo, int64_t B, int64_t T, int64_t N,
                                        int64_t a_stride_t) {
     if (!dtype_ok(dtype) || !sizes_ok(B, T, N)) return 0;
@@ -141,6 +148,29 @@ int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A, co
                                  a_stride_b, a_stride_t, workspace, workspace_bytes, s);
     return backward_t<double>(algo, grad_y, A, zi, y, grad_x, grad_A, grad_zi, B, T, N,
                               a_stride_b, a_stride_t, workspace, workspace_bytes, s);
+}
+
+int lpc_b200_workspace_status(const void *workspace, unsigned *status, void *stream) {
+    if (!workspace || !status) return LPC_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the status word follows the ticket counter in the workspace header
+    if (cudaMemcpyAsync(status, static_cast<const unsigned char *>(workspace) + sizeof(unsigned), sizeof(unsigned),
+                        cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return LPC_ERR_CUDA;
+    return cudaStreamSynchronize(s) == cudaSuccess ? LPC_OK : LPC_ERR_CUDA;
+}
+
+size_t lpc_b200_selftest_workspace_size(void) { return chunked_selftest_workspace(); }
+
+int lpc_b200_selftest_timeout(void *workspace, size_t workspace_bytes, unsigned spin_limit, unsigned *status,
+                              void *stream) {
+    if (!workspace || !status || spin_limit == 0) return LPC_ERR_INVALID_ARGUMENT;
+    if (workspace_bytes < chunked_selftest_workspace()) return LPC_ERR_WORKSPACE;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (chunked_selftest_timeout(workspace, workspace_bytes, spin_limit, s) != cudaSuccess) return LPC_ERR_CUDA;
+    const int rc = lpc_b200_workspace_status(workspace, status, stream);
+    if (rc != LPC_OK) return rc;
+    return *status != 0u ? LPC_ERR_TIMEOUT : LPC_OK;
 }
 
 size_t lpc_b200_ragged_workspace_size(int dtype, int64_t nsig, int64_t S, int64_t N) {

@@ -38,6 +38,8 @@
 // fused into the phase-D epilogue (time-invariant A: a separate reduction
 // kernel over the grad_x just written); grad_zi is the adjoint carried N steps
 // past t = 0.
+#include <atomic>
+
 #include "lpc_chunked.cuh"
 #include "lpc_ti.cuh"
 
@@ -993,7 +995,10 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
 // ----------------------------------------------------------------------------
 // Host side.
 // ----------------------------------------------------------------------------
-constexpr int kChunkLen = 256;   // target chunk length; rounded to an even number of windows
+constexpr int kChunkLen = 256;   // default target chunk length; rounded to an even number of windows
+
+// Process-wide target chunk length (the autotuner's knob; 0 = default).
+std::atomic<int64_t> g_chunk_target{0};
 constexpr int kMaxChunksPerBatch = 64;
 
 inline int threads_for(int) { return 256; }  // scan group: one group of N+1 lanes per chunk
@@ -1011,7 +1016,9 @@ inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N) {
     Plan pl;
     pl.NP = padded_order(N);
     const int W = window_for(pl.NP);
-    pl.L = 2 * W * ((kChunkLen + 2 * W - 1) / (2 * W));  // an even number of windows: halves split on one
+    const int64_t want = g_chunk_target.load(std::memory_order_relaxed);
+    const int64_t target = want > 0 ? want : kChunkLen;
+    pl.L = (int)(2 * W * ((target + 2 * W - 1) / (2 * W)));  // an even number of windows: halves split on one
     int G = (int)(threads_for(pl.NP) / (N + 1));
     if (G > kMaxChunksPerBatch) G = kMaxChunksPerBatch;
     const int ctas = esz == 4 ? (pl.NP <= 16 ? 4 : 3) : 2;
@@ -1097,6 +1104,16 @@ ChunkParams<T> base_params(const Plan &pl, int64_t B, int64_t T_, int64_t N, voi
 }  // namespace
 
 bool chunked_supported(int64_t N) { return N >= 1 && N <= 32; }
+
+void set_chunk_target(int64_t samples) {
+    g_chunk_target.store(samples <= 0 ? 0 : (samples < 32 ? 32 : (samples > 4096 ? 4096 : samples)),
+                         std::memory_order_relaxed);
+}
+
+int64_t chunk_target() {
+    const int64_t v = g_chunk_target.load(std::memory_order_relaxed);
+    return v > 0 ? v : kChunkLen;
+}
 
 bool chunked_preferred(int64_t B, int64_t T, int64_t N, int64_t a_stride_t) {
     if (!chunked_supported(N) || a_stride_t == 0) return false;
@@ -1299,6 +1316,46 @@ template cudaError_t chunked_backward_ragged<float>(const float *, const float *
 template cudaError_t chunked_backward_ragged<double>(const double *, const double *, const int64_t *,
                                                      const double *, const double *, double *, double *, double *,
                                                      int64_t, int64_t, int64_t, void *, size_t, cudaStream_t);
+
+// ----------------------------------------------------------------------------
+// Failure detection without a fault: a chunked forward whose ticket queue
+// starts past batch 0, so batch 1's look-back waits for a flag nothing ever
+// sets.  With a short spin limit the wait gives up, records
+// kStatusFlagWait in the status word and the kernel finishes normally.
+// ----------------------------------------------------------------------------
+size_t chunked_selftest_workspace() {
+    const int64_t N = 2;
+    const Plan pl = make_plan(4, 1, 1, N);
+    const int64_t T = 2 * (int64_t)pl.G * pl.L;  // two batches
+    return ws_layout(4, 2, N).total + align256((size_t)(2 * T + T * N) * sizeof(float));
+}
+
+cudaError_t chunked_selftest_timeout(void *ws, size_t ws_bytes, unsigned spin_limit, cudaStream_t st) {
+    const int64_t N = 2;
+    const Plan pl = make_plan(4, 1, 1, N);
+    const int64_t T = 2 * (int64_t)pl.G * pl.L;
+    const Plan p2 = make_plan(4, 1, T, N);
+    if (ws_bytes < chunked_selftest_workspace() || p2.nbatches != 2) return cudaErrorInvalidValue;
+    const WsLayout l = ws_layout(4, p2.nbatches, N);
+    float *x = reinterpret_cast<float *>(static_cast<unsigned char *>(ws) + l.total);
+    float *y = x + T;
+    float *A = y + T;
+    cudaError_t e = cudaMemsetAsync(ws, 0, chunked_selftest_workspace(), st);  // zero inputs, header, flags
+    if (e != cudaSuccess) return e;
+    const unsigned first = 1;  // skip batch 0: its flag is never published
+    e = cudaMemcpyAsync(ws, &first, sizeof(first), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    ChunkParams<float> p = base_params<float>(p2, 1, T, N, ws);
+    p.in = x;
+    p.A = A;
+    p.as_b = T * N;
+    p.as_t = N;
+    p.out = y;
+    p.spin_limit = spin_limit;
+    e = dispatch<float, false, false>(p, p2.NP, st);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);  // `first` lives on this host stack frame
+}
 
 template cudaError_t chunked_forward<float>(const FwdArgs<float> &, bool, void *, size_t, cudaStream_t);
 template cudaError_t chunked_forward<double>(const FwdArgs<double> &, bool, void *, size_t, cudaStream_t);

@@ -10,6 +10,10 @@ namespace lpcb {
 constexpr int64_t kMaxOrder = 1024;
 
 bool chunked_supported(int64_t N);
+// Target chunk length of the chunked scan (process-wide; <= 0 restores the
+// default); the plan rounds it to an even number of windows.
+void set_chunk_target(int64_t samples);
+int64_t chunk_target();
 bool chunked_preferred(int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
 size_t chunked_forward_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
 size_t chunked_backward_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
@@ -23,6 +27,10 @@ template <typename T>
 cudaError_t chunked_backward_ragged(const T *gy, const T *A, const int64_t *off, const T *zi, const T *y, T *gx,
                                     T *gA, T *gzi, int64_t nsig, int64_t S, int64_t N, void *ws, size_t ws_bytes,
                                     cudaStream_t st);
+
+// Failure detection: a launch whose look-back wait runs out (no GPU fault).
+size_t chunked_selftest_workspace();
+cudaError_t chunked_selftest_timeout(void *ws, size_t ws_bytes, unsigned spin_limit, cudaStream_t st);
 
 template <typename T>
 cudaError_t chunked_forward(const FwdArgs<T> &p, bool neg, void *ws, size_t ws_bytes,
