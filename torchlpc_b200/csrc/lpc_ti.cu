@@ -129,8 +129,10 @@ __global__ void __launch_bounds__(256) ti_power_kernel(const T *a, int64_t as_b,
 // ---------------------------------------------------------------- zero / fix
 // FIX = false: chunk from zero state, exit state to zst.  FIX = true: chunk
 // from its entry state est, outputs written.  REV: time runs backwards
-// (index T-1-s of in/out for step s).
-template <typename T, int NP, bool REV, bool FIX>
+// (index T-1-s of in/out for step s).  VEC (T a multiple of 4 floats, 16-byte
+// aligned rows): each thread's input and output stream moves in 16-byte
+// groups of 4 steps, the next group's load issued one group ahead.
+template <typename T, int NP, bool REV, bool FIX, bool VEC>
 __global__ void __launch_bounds__(256) ti_chunk_kernel(TiArgs<T> p) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= p.B * p.nc) return;
@@ -152,18 +154,53 @@ __global__ void __launch_bounds__(256) ti_chunk_kernel(TiArgs<T> p) {
     const T *inb = p.in + b * p.T;
     T *outb = p.out + b * p.T;
     const int64_t s0 = c * p.Lc;
-    const int nblk = (int)((min64(p.Lc, p.T - s0) + NP - 1) / NP);  // blocks holding samples
+    const int64_t send = min64(s0 + p.Lc, p.T);  // steps holding samples end here
+    const int nblk = (int)((send - s0 + NP - 1) / NP);
+    if constexpr (VEC && sizeof(T) == 4 && NP % 4 == 0) {
+        // groups of 4 steps s..s+3: forward elements t..t+3, backward t-3..t
+        auto gload = [&](int64_t s) -> float4 {
+            if (s >= send) return make_float4(0.f, 0.f, 0.f, 0.f);
+            const int64_t t = REV ? p.T - 4 - s : s;
+            return *reinterpret_cast<const float4 *>(inb + t);
+        };
+        float4 nxt = gload(s0);
 #pragma unroll 1
-    for (int blk = 0; blk < nblk; ++blk) {
-        const int64_t sb = s0 + (int64_t)blk * NP;
+        for (int blk = 0; blk < nblk; ++blk) {
+            const int64_t sb = s0 + (int64_t)blk * NP;
 #pragma unroll
-        for (int u = 0; u < NP; ++u) {
-            const int64_t s = sb + u;
-            const bool in_range = s < p.T;
-            const int64_t t = REV ? p.T - 1 - s : s;
-            const T xv = in_range ? inb[t] : T(0);
-            h[u] = ti_step<T, NP>(a, h, u, xv);
-            if (FIX && in_range) outb[t] = h[u];
+            for (int g = 0; g < NP / 4; ++g) {
+                const float4 cur = nxt;
+                nxt = gload(sb + 4 * g + 4);
+                const float xin[4] = {REV ? cur.w : cur.x, REV ? cur.z : cur.y, REV ? cur.y : cur.z,
+                                      REV ? cur.x : cur.w};
+                float o[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int u = 4 * g + k;
+                    h[u] = ti_step<T, NP>(a, h, u, xin[k]);
+                    o[k] = h[u];
+                }
+                const int64_t s = sb + 4 * g;
+                if (FIX && s < send) {
+                    const int64_t t = REV ? p.T - 4 - s : s;
+                    *reinterpret_cast<float4 *>(outb + t) =
+                        REV ? make_float4(o[3], o[2], o[1], o[0]) : make_float4(o[0], o[1], o[2], o[3]);
+                }
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int blk = 0; blk < nblk; ++blk) {
+            const int64_t sb = s0 + (int64_t)blk * NP;
+#pragma unroll
+            for (int u = 0; u < NP; ++u) {
+                const int64_t s = sb + u;
+                const bool in_range = s < send;
+                const int64_t t = REV ? p.T - 1 - s : s;
+                const T xv = in_range ? inb[t] : T(0);
+                h[u] = ti_step<T, NP>(a, h, u, xv);
+                if (FIX && in_range) outb[t] = h[u];
+            }
         }
     }
     if constexpr (!FIX) {
@@ -259,9 +296,19 @@ cudaError_t ti_run(TiArgs<T> p, cudaStream_t st) {
     ti_power_kernel<T, NP><<<(unsigned)p.B, 256, 0, st>>>(p.a, p.as_b, p.N, p.Lc, p.P);
     const int64_t threads = p.B * p.nc;
     const unsigned g1 = (unsigned)((threads + 255) / 256);
-    ti_chunk_kernel<T, NP, REV, false><<<g1, 256, 0, st>>>(p);
+    // 16-byte groups need whole groups per signal, aligned rows and an order
+    // that is a multiple of the group
+    const bool vec = sizeof(T) == 4 && NP % 4 == 0 && p.T % 4 == 0 &&
+                     (reinterpret_cast<uintptr_t>(p.in) & 15u) == 0 && (reinterpret_cast<uintptr_t>(p.out) & 15u) == 0;
+    if (vec)
+        ti_chunk_kernel<T, NP, REV, false, true><<<g1, 256, 0, st>>>(p);
+    else
+        ti_chunk_kernel<T, NP, REV, false, false><<<g1, 256, 0, st>>>(p);
     ti_combine_kernel<T, NP, REV><<<(unsigned)((p.B * 32 + 255) / 256), 256, 0, st>>>(p);
-    ti_chunk_kernel<T, NP, REV, true><<<g1, 256, 0, st>>>(p);
+    if (vec)
+        ti_chunk_kernel<T, NP, REV, true, true><<<g1, 256, 0, st>>>(p);
+    else
+        ti_chunk_kernel<T, NP, REV, true, false><<<g1, 256, 0, st>>>(p);
     return cudaGetLastError();
 }
 
