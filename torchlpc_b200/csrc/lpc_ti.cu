@@ -237,44 +237,83 @@ __global__ void __launch_bounds__(256) ti_combine_kernel(TiArgs<T> p) {
 
 // ---------------------------------------------------------------- gradients
 // grad_a[b,i] = sgn * sum_t grad_x[b,t] * ypad[b,t-1-i], ypad(-1-k) = zi[b,k].
-template <typename T, int NP>
+// One thread per segment of a signal keeps the last NP outputs in a register
+// ring (slot (i - j) mod NP holds y[t_j - 1 - i] at step j), so each sample
+// costs one load of grad_x, one of y and NP FMAs; warps whose lanes share a
+// signal reduce with shuffles and add once per tap.  VEC: 16-byte loads.
+template <typename T, int NP, bool VEC>
 __global__ void __launch_bounds__(256) ti_grad_a_kernel(const T *gx, const T *y, const T *zi, T *ga, int64_t B,
-                                                       int64_t T_, int N, T sgn) {
-    __shared__ T part[8][NP];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
+                                                       int64_t T_, int N, int seg, int64_t nseg, T sgn) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool on = idx < B * nseg;
+    const int64_t b = on ? idx / nseg : -1;
+    T acc[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) acc[i] = T(0);
+    if (on) {
+        const int64_t t0 = (idx - b * nseg) * seg;
+        const int64_t tend = min64(t0 + seg, T_);
         const T *gb = gx + b * T_;
         const T *yb = y + b * T_;
         const T *zb = zi ? zi + b * N : nullptr;
-        T acc[NP];
+        T yr[NP];
 #pragma unroll
-        for (int i = 0; i < NP; ++i) acc[i] = T(0);
-        for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T_;
-             t += (int64_t)gridDim.x * blockDim.x) {
-            const T g = gb[t];
+        for (int i = 0; i < NP; ++i) {
+            const int64_t j = t0 - 1 - i;
+            yr[i] = j >= 0 ? yb[j] : ((zb && -1 - j < N) ? zb[-1 - j] : T(0));
+        }
+        const int nblk = (int)((tend - t0 + NP - 1) / NP);
+#pragma unroll 1
+        for (int blk = 0; blk < nblk; ++blk) {
+            const int64_t tb = t0 + (int64_t)blk * NP;
+            if constexpr (VEC && sizeof(T) == 4 && NP % 4 == 0) {
 #pragma unroll
-            for (int i = 0; i < NP; ++i) {
-                if (i < N) {
-                    const int64_t j = t - 1 - i;
-                    const T yy = j >= 0 ? yb[j] : ((zb && i - t < N) ? zb[i - t] : T(0));
-                    acc[i] = fma(g, yy, acc[i]);
+                for (int q = 0; q < NP / 4; ++q) {
+                    const int64_t t = tb + 4 * q;
+                    float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f), y4 = g4;
+                    if (t < tend) {
+                        g4 = *reinterpret_cast<const float4 *>(gb + t);
+                        y4 = *reinterpret_cast<const float4 *>(yb + t);
+                    }
+                    const float gv[4] = {g4.x, g4.y, g4.z, g4.w};
+                    const float yv[4] = {y4.x, y4.y, y4.z, y4.w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int u = 4 * q + k;
+#pragma unroll
+                        for (int i = 0; i < NP; ++i) acc[i] = fma(gv[k], yr[(i - u + NP) % NP], acc[i]);
+                        yr[NP - 1 - u] = yv[k];
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < NP; ++u) {
+                    const int64_t t = tb + u;
+                    const T g = t < tend ? gb[t] : T(0);
+#pragma unroll
+                    for (int i = 0; i < NP; ++i) acc[i] = fma(g, yr[(i - u + NP) % NP], acc[i]);
+                    yr[NP - 1 - u] = t < T_ ? yb[t] : T(0);
                 }
             }
         }
+    }
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    // every lane takes part in both collectives (idle lanes included)
+    const int64_t b0 = __shfl_sync(full, b, 0);
+    const bool uniform = __all_sync(full, on && b == b0);
+    if (uniform) {
 #pragma unroll
         for (int i = 0; i < NP; ++i) {
             T v = acc[i];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) part[warp][i] = v;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(full, v, o);
+            if (lane == 0 && i < N && v != T(0)) atomicAdd(ga + b * N + i, sgn * v);
         }
-        __syncthreads();
-        if (threadIdx.x < N && threadIdx.x < NP) {
-            T v = T(0);
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += part[w][threadIdx.x];
-            if (v != T(0)) atomicAdd(ga + b * N + threadIdx.x, sgn * v);
-        }
-        __syncthreads();
+    } else if (on) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+            if (i < N && acc[i] != T(0)) atomicAdd(ga + b * N + i, sgn * acc[i]);
     }
 }
 
@@ -347,10 +386,16 @@ TiArgs<T> ti_args(const TiLayout &l, const T *in, const T *a, int64_t as_b, cons
 template <typename T, int NP>
 cudaError_t launch_grad_a(const T *gx, const T *y, const T *zi, T *ga, int64_t B, int64_t T_, int N, T sgn,
                           cudaStream_t st) {
-    const int64_t per_block = 256 * 64;  // samples a block covers per signal
-    const unsigned gxd = (unsigned)min64(4096, (T_ + per_block - 1) / per_block);
-    const unsigned gyd = (unsigned)min64(65535, B);
-    ti_grad_a_kernel<T, NP><<<dim3(gxd, gyd), 256, 0, st>>>(gx, y, zi, ga, B, T_, N, sgn);
+    const int seg = ti_chunk_len(NP);
+    const int64_t nseg = (T_ + seg - 1) / seg;
+    const int64_t threads = B * nseg;
+    const unsigned grid = (unsigned)((threads + 255) / 256);
+    const bool vec = sizeof(T) == 4 && NP % 4 == 0 && T_ % 4 == 0 && (reinterpret_cast<uintptr_t>(gx) & 15u) == 0 &&
+                     (reinterpret_cast<uintptr_t>(y) & 15u) == 0;
+    if (vec)
+        ti_grad_a_kernel<T, NP, true><<<grid, 256, 0, st>>>(gx, y, zi, ga, B, T_, N, seg, nseg, sgn);
+    else
+        ti_grad_a_kernel<T, NP, false><<<grid, 256, 0, st>>>(gx, y, zi, ga, B, T_, N, seg, nseg, sgn);
     return cudaGetLastError();
 }
 
