@@ -58,10 +58,12 @@ const char *lpc_b200_status_string(int status);
 int lpc_b200_version(void);
 
 /* Target chunk length (samples) of the chunked scan, process-wide: the
- * autotuner's knob (no reference counterpart).  <= 0 restores the default
- * (256); values are clamped to [32, 4096] and rounded up to an even number of
- * the kernel's windows.  Workspace sizes follow the current setting, so change
- * it only between calls. */
+ * autotuner's knob (no reference counterpart).  <= 0 restores the default,
+ * chosen per call by signal length (128 below 65,536 samples, 256 below 2^19,
+ * 512 from there; 1024 for ragged batches), and lpc_b200_chunk_length
+ * then returns 0.  Values are clamped to [32, 4096] and rounded up to an even
+ * number of the kernel's windows.  Workspace sizes follow the current
+ * setting, so change it only between calls. */
 int lpc_b200_set_chunk_length(int64_t samples);
 int64_t lpc_b200_chunk_length(void);
 
@@ -107,8 +109,8 @@ int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A,
  * Runs the chunked kernel with scratch taken from an 8 MiB array compiled
  * into this library (held on every GPU that loads it, until exit).  Returns
  * LPC_ERR_WORKSPACE when the problem needs more scratch than that (roughly
- * 23 million samples per call at order 16), LPC_ERR_UNSUPPORTED for orders
- * above 32.  The first call on a device looks up the array's device address
+ * 12 to 47 million samples per call at order 16, more for longer signals),
+ * LPC_ERR_UNSUPPORTED for orders above 32.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * Every call shares the one array: calls whose work overlaps on the GPU
  * (different streams, or several host threads) race and must be serialised

@@ -46,6 +46,7 @@ def set_chunk_length(samples: int) -> None:
 
 
 def get_chunk_length() -> int:
+    """The chunk-length setting (0: chosen per call by signal length)."""
     _require()
     return int(_lib().lpc_b200_chunk_length())
 

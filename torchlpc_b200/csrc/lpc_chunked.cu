@@ -995,7 +995,11 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_ke
 // ----------------------------------------------------------------------------
 // Host side.
 // ----------------------------------------------------------------------------
-constexpr int kChunkLen = 256;   // default target chunk length; rounded to an even number of windows
+constexpr int kChunkLen = 256;   // target chunk length for mid-length signals (rounded to an even number of windows)
+
+// Default target chunk length by signal length (measured on B200: 128 for
+// 16,000-sample signals, 512 for 2^20-sample signals).
+inline int64_t default_chunk(int64_t T) { return T < 65536 ? kChunkLen / 2 : (T < (1 << 19) ? kChunkLen : 2 * kChunkLen); }
 
 // Process-wide target chunk length (the autotuner's knob; 0 = default).
 std::atomic<int64_t> g_chunk_target{0};
@@ -1012,12 +1016,14 @@ struct Plan {
 // Chunks per batch: one group of N+1 lanes per chunk, capped so that the
 // shared memory of a CTA fits the occupancy the kernel is built for (fp32:
 // four CTAs per SM up to order 16, three above; fp64: two).
-inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N) {
+inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N, int64_t dflt = 0) {
     Plan pl;
     pl.NP = padded_order(N);
     const int W = window_for(pl.NP);
     const int64_t want = g_chunk_target.load(std::memory_order_relaxed);
-    const int64_t target = want > 0 ? want : kChunkLen;
+    // default by signal length: short signals want more batches in flight,
+    // long ones fewer look-back hops per sample
+    const int64_t target = want > 0 ? want : (dflt > 0 ? dflt : default_chunk(T));
     pl.L = (int)(2 * W * ((target + 2 * W - 1) / (2 * W)));  // an even number of windows: halves split on one
     int G = (int)(threads_for(pl.NP) / (N + 1));
     if (G > kMaxChunksPerBatch) G = kMaxChunksPerBatch;
@@ -1110,10 +1116,7 @@ void set_chunk_target(int64_t samples) {
                          std::memory_order_relaxed);
 }
 
-int64_t chunk_target() {
-    const int64_t v = g_chunk_target.load(std::memory_order_relaxed);
-    return v > 0 ? v : kChunkLen;
-}
+int64_t chunk_target() { return g_chunk_target.load(std::memory_order_relaxed); }
 
 bool chunked_preferred(int64_t B, int64_t T, int64_t N, int64_t a_stride_t) {
     if (!chunked_supported(N) || a_stride_t == 0) return false;
@@ -1225,7 +1228,10 @@ struct RaggedLayout {
 
 inline RaggedLayout ragged_layout(size_t esz, int64_t nsig, int64_t S, int64_t N) {
     RaggedLayout r;
-    r.pl = make_plan(esz, 1, 1, N);  // chunk length and batch size depend on the order only
+    // ragged batches are numbered signal by signal, so a signal's batches run
+    // side by side and look back over each other: long chunks (fewer batches,
+    // 1024 samples measured best on B200) unless the caller set a length
+    r.pl = make_plan(esz, 1, int64_t(1) << 20, N, 4 * kChunkLen);
     const int64_t span = (int64_t)r.pl.G * r.pl.L;
     r.nbmax = nsig + S / span + 1;
     r.l = ws_layout(esz, r.nbmax, N);

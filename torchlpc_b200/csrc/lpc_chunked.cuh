@@ -11,7 +11,8 @@ constexpr int64_t kMaxOrder = 1024;
 
 bool chunked_supported(int64_t N);
 // Target chunk length of the chunked scan (process-wide; <= 0 restores the
-// default); the plan rounds it to an even number of windows.
+// default, chosen by signal length; chunk_target() then returns 0); the plan
+// rounds it to an even number of windows.
 void set_chunk_target(int64_t samples);
 int64_t chunk_target();
 bool chunked_preferred(int64_t B, int64_t T, int64_t N, int64_t a_stride_t);
