@@ -13,11 +13,11 @@ from typing import Optional, Tuple, Union
 import torch
 
 from ._ops import EXTENSION_LOADED, available_algos, get_algo, set_algo
-from .core import LPC, LPCRagged
+from .core import LPC, LPCCheckpointed, LPCRagged
 from .recurrence import Recurrence
 
 __all__ = ["sample_wise_lpc", "linear_recurrence", "LPC", "Recurrence", "EXTENSION_LOADED",
-           "set_algo", "get_algo", "available_algos", "sample_wise_lpc_ragged", "LPCRagged"]
+           "set_algo", "get_algo", "available_algos", "sample_wise_lpc_ragged", "LPCRagged", "set_checkpoint_segment", "LPCCheckpointed"]
 
 
 def linear_recurrence(a: torch.Tensor, x: torch.Tensor, zi: Optional[torch.Tensor] = None) -> torch.Tensor:
@@ -64,6 +64,23 @@ def _time_invariant_source(a: torch.Tensor) -> Optional[torch.Tensor]:
     return None
 
 
+_CHECKPOINT_SEGMENT = 0
+
+
+def set_checkpoint_segment(samples: int) -> None:
+    """Boundary-state checkpointing for long signals: when ``samples`` > 0,
+    ``sample_wise_lpc`` on signals longer than that keeps the N-sample state
+    entering every segment of ``samples`` samples instead of the output y, and
+    its backward recomputes y segment by segment (``LPCCheckpointed``).  0
+    (the default) turns it off; segments shorter than the filter order are not
+    checkpointed.  For plain reverse-mode autograd (no forward AD, vmap or
+    double backward through the checkpointed filter).
+    """
+    global _CHECKPOINT_SEGMENT
+    assert samples >= 0
+    _CHECKPOINT_SEGMENT = int(samples)
+
+
 def sample_wise_lpc(
     x: torch.Tensor,
     a: torch.Tensor,
@@ -92,7 +109,11 @@ def sample_wise_lpc(
         y = linear_recurrence(-a.squeeze(2), x, zi.squeeze(1))
     else:
         src = _time_invariant_source(a)
-        y = LPC.apply(x, src if src is not None else a, zi)
+        A = src if src is not None else a
+        if _CHECKPOINT_SEGMENT and T > _CHECKPOINT_SEGMENT >= order:
+            y = LPCCheckpointed.apply(x, A, zi, _CHECKPOINT_SEGMENT)
+        else:
+            y = LPC.apply(x, A, zi)
 
     if return_zf:
         return y, y[:, -order:].flip(1)

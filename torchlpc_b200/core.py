@@ -122,3 +122,67 @@ class LPCRagged(Function):
         needs = ctx.needs_input_grad
         gx, gA, gzi = _ops.lpc_backward_ragged(grad_y, A, offsets, zi, y, bool(needs[1]), bool(needs[3]))
         return (gx if needs[0] else None, gA if needs[1] else None, None, gzi if needs[3] else None)
+
+
+class LPCCheckpointed(Function):
+    """The filter with boundary-state checkpointing for long signals.
+
+    ``LPCCheckpointed.apply(x, A, zi, segment)``: same result as
+    ``LPC.apply(x, A, zi)``, but instead of the output y (B,T) it keeps the
+    N-sample state entering every segment of ``segment`` samples (torchlpc's
+    LPC saves y, core.py:179-184).  The backward walks the segments from last
+    to first: it recomputes a segment's outputs from its saved entry state (one
+    forward call), runs the fused backward on it, and carries the adjoint of the
+    segment's entry state (its grad_zi) into the last N output gradients of the
+    segment before it.  Costs one extra forward pass; keeps x instead of y, so
+    it saves memory when the caller holds x anyway; y then exists only for one
+    segment at a time during the backward.  Not itself differentiable.
+    """
+
+    @staticmethod
+    def forward(x: torch.Tensor, A: torch.Tensor, zi: torch.Tensor, segment: int) -> torch.Tensor:
+        return _ops.lpc(x, A, zi)
+
+    @staticmethod
+    def setup_context(ctx: Any, inputs: List[Any], output: Any) -> Any:
+        x, A, zi, segment = inputs
+        y = output
+        N = A.shape[-1]
+        T = y.shape[1]
+        # entry state of segment k >= 1: zi convention, state[j] = y[s-1-j]
+        states = [zi] + [y[:, s - N:s].flip(1) for s in range(segment, T, segment)]
+        ctx.save_for_backward(x, A, zi, torch.stack(states))
+        ctx.segment = segment
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx: Any, grad_y: torch.Tensor):
+        x, A, zi, states = ctx.saved_tensors
+        needs = ctx.needs_input_grad
+        seg = ctx.segment
+        B, T = x.shape
+        N = A.shape[-1]
+        ti = A.dim() == 2
+        gx = torch.empty_like(x) if needs[0] else None
+        gA = (torch.zeros_like(A) if ti else torch.empty_like(A)) if needs[1] else None
+        carry = None  # grad_zi of the segment after the current one
+        starts = list(range(0, T, seg))
+        for k in reversed(range(len(starts))):
+            s = starts[k]
+            e = min(s + seg, T)
+            Ak = A if ti else A[:, s:e]
+            zk = states[k]
+            yk = _ops.lpc(x[:, s:e].contiguous(), Ak, zk)
+            gyk = grad_y[:, s:e].contiguous()
+            if carry is not None:  # the next segment starts from this one's last N outputs
+                gyk = gyk.clone()
+                gyk[:, -N:] += carry.flip(1)
+            gxk, gAk, carry = _ops.lpc_backward(gyk, Ak, zk, yk, gA is not None, True)
+            if gx is not None:
+                gx[:, s:e] = gxk
+            if gA is not None:
+                if ti:
+                    gA += gAk
+                else:
+                    gA[:, s:e] = gAk
+        return gx, gA, carry if needs[2] else None, None
