@@ -424,6 +424,33 @@ def run_reference(args):
     return 0
 
 
+def other_configs(tl, headline: str, device) -> dict:
+    """fwd+bwd samples/s of the other workloads at their full sizes (operator
+    level, CUDA events; the default algorithm, and the plain kernel where it
+    finishes in seconds), outside the timed region of the headline."""
+    out = {}
+    for cfg in ("cfg2", "cfg4", "cfg5"):
+        if cfg == headline:
+            continue
+        w = load_workload(cfg, device)
+        if w["workload"].ragged:
+            w["offsets_dev"] = w["offsets"].to(device)
+        S = samples_of(w)
+        x, A, zi, gy = w["x"], w["A"], w["zi"], w["gy"]
+        entry = {"samples_per_step": S, "note": w["workload"].note}
+        for algo in ("auto", "plain"):
+            if algo == "plain" and w["workload"].ragged:
+                continue
+            tl.set_algo(algo)
+            tf, tb = kernel_times(tl, w, x, A, zi, gy, 3 if algo == "plain" else 10, device)
+            entry[algo] = {"GS_per_s": S / ((tf + tb) * 1e-3) / 1e9, "fwd_ms": tf, "bwd_ms": tb}
+        tl.set_algo("auto")
+        out[cfg] = entry
+        del w, x, A, zi, gy
+        torch.cuda.empty_cache()
+    return out
+
+
 # --------------------------------------------------------------------------- main
 def run_ours(args):
     ws, rk, lr = rank_info()
@@ -492,6 +519,9 @@ def run_ours(args):
             line["plain"] = {"value": S / (msp * 1e-3), "ms_per_step": msp,
                              "speedup": msp / ms}
         line["max_rel_err_vs_fp64"] = accuracy(tl, w, x, A, zi, gy, args.algo)
+        if not args.no_extras and ws == 1:
+            line["other_configs"] = other_configs(tl, args.config, device)
+            tl.set_algo(args.algo)
         if not args.no_e2e:
             ems, h2d, d2h = e2e_time(tl, w, x, A, zi, gy, max(3, args.steps // 4), 2, device)
             line["e2e"] = {"value": S / (ems * 1e-3), "unit": "samples/s", "ms_per_step": ems,
