@@ -109,7 +109,7 @@ int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A,
  * Runs the chunked kernel with scratch taken from an 8 MiB array compiled
  * into this library (held on every GPU that loads it, until exit).  Returns
  * LPC_ERR_WORKSPACE when the problem needs more scratch than that (roughly
- * 12 to 47 million samples per call at order 16, more for longer signals),
+ * 13 to 50 million samples per call at order 16, more for longer signals),
  * LPC_ERR_UNSUPPORTED for orders above 32.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * Every call shares the one array: calls whose work overlaps on the GPU

@@ -146,10 +146,19 @@ struct Sig {
     int vx;          // input windows move as 16-byte vectors
 };
 
+// Steps per phase-A window (phase D: half of it): orders up to 16 stage 32
+// steps per barrier at two CTAs per SM, larger orders 16+ steps at three
+// (measured on B200: the longer window shortens the backward by ~11 % at
+// order 16 and slows order 24).
+__host__ __device__ constexpr int window_steps(int NP) {
+    return (NP <= 16 ? 2 : 1) * NP * ((16 + NP - 1) / NP);
+}
+__host__ __device__ constexpr int ctas_per_sm(int NP, int esz) { return esz == 4 && NP > 16 ? 3 : 2; }
+
 template <int NP>
 struct Cfg {
     static constexpr int THREADS = 256;
-    static constexpr int W = NP * ((16 + NP - 1) / NP);  // phase-A window: steps, a multiple of NP
+    static constexpr int W = window_steps(NP);           // phase-A window: steps, a multiple of NP
     static constexpr int WD = W / 2;                     // phase-D window (half-chunks, half the steps)
 };
 
@@ -235,7 +244,7 @@ struct SmemPlan {
     size_t abuf, ibuf, obuf, ybuf, maps, half, st, sin, lbP, lbz, misc, total;
     __host__ __device__ SmemPlan(size_t esz, int NP, int G, bool rev) {
         auto al = [](size_t v) { return (v + 15) & ~size_t(15); };
-        const int W = NP * ((16 + NP - 1) / NP), WD = W / 2;
+        const int W = window_steps(NP), WD = W / 2;
         size_t off = 0;
         abuf = off;
         const size_t awin = al((size_t)2 * G * group_stride(W, NP, (int)esz) * esz);
@@ -487,7 +496,7 @@ __device__ __forceinline__ void fix_steps(const T *Ag, const T *xg, T *og, int j
 // The kernel.
 // ----------------------------------------------------------------------------
 template <typename T, int NP, bool REV, bool NEG>
-__global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 4 : 3) chunked_kernel(ChunkParams<T> p) {
+__global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_kernel(ChunkParams<T> p) {
     constexpr int W = Cfg<NP>::W;
     constexpr int WD = Cfg<NP>::WD;
     constexpr int THREADS = Cfg<NP>::THREADS;
@@ -1006,7 +1015,7 @@ std::atomic<int64_t> g_chunk_target{0};
 constexpr int kMaxChunksPerBatch = 64;
 
 inline int threads_for(int) { return 256; }  // scan group: one group of N+1 lanes per chunk
-inline int window_for(int NP) { return NP * ((16 + NP - 1) / NP); }
+inline int window_for(int NP) { return window_steps(NP); }
 
 struct Plan {
     int NP, G, L;
@@ -1014,8 +1023,8 @@ struct Plan {
 };
 
 // Chunks per batch: one group of N+1 lanes per chunk, capped so that the
-// shared memory of a CTA fits the occupancy the kernel is built for (fp32:
-// four CTAs per SM up to order 16, three above; fp64: two).
+// shared memory of a CTA fits the occupancy the kernel is built for
+// (ctas_per_sm: two CTAs per SM up to order 16 and for fp64, three above).
 inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N, int64_t dflt = 0) {
     Plan pl;
     pl.NP = padded_order(N);
@@ -1027,7 +1036,7 @@ inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N, int64_t dflt 
     pl.L = (int)(2 * W * ((target + 2 * W - 1) / (2 * W)));  // an even number of windows: halves split on one
     int G = (int)(threads_for(pl.NP) / (N + 1));
     if (G > kMaxChunksPerBatch) G = kMaxChunksPerBatch;
-    const int ctas = esz == 4 ? (pl.NP <= 16 ? 4 : 3) : 2;
+    const int ctas = ctas_per_sm(pl.NP, (int)esz);
     const size_t budget = (size_t)228 * 1024 / ctas - 1024;  // per-SM shared memory less the per-CTA reserve
     while (G > 1 && SmemPlan(esz, pl.NP, G, true).total > budget) --G;
     pl.G = G;

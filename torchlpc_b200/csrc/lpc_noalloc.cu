@@ -23,7 +23,7 @@ using namespace lpcb;
 
 namespace {
 
-// 8 MiB: enough for about 6,500 batches of chunks, i.e. roughly 12 to 47
+// 8 MiB: enough for about 6,500 batches of chunks, i.e. roughly 13 to 50
 // million samples per call at order 16 (longer signals use longer chunks; the
 // scratch grows with the number of batches and with N^2).
 constexpr size_t kStaticScratchBytes = size_t(8) << 20;
