@@ -443,10 +443,12 @@ struct Loader {
     }
 };
 
-// Phase A: NS steps of one window segment of a chunk-map lane (ring
-// positions U0..U0+NS-1), slots jbase.. of the window.
-template <typename T, int NP, bool REV, bool NEG, int WC, int U0, int NS>
-__device__ __forceinline__ void map_steps(const T *Ag, const T *xg, bool xlane, int jbase, T (&h)[NP]) {
+// Phase A: NS steps of one window segment of a chunk-map lane running KF
+// filters (ring positions U0..U0+NS-1), slots jbase.. of the window.  Bit q of
+// xmask marks filter q as the zero-state filter (the one fed the input).  One
+// broadcast load of a coefficient row feeds all KF filters of the lane.
+template <typename T, int NP, int KF, bool REV, bool NEG, int WC, int U0, int NS>
+__device__ __forceinline__ void map_steps(const T *Ag, const T *xg, unsigned xmask, int jbase, T (&h)[KF][NP]) {
 #pragma unroll
     for (int j = 0; j < NS; ++j) {
         const int u = (U0 + j) % NP;
@@ -458,11 +460,38 @@ __device__ __forceinline__ void map_steps(const T *Ag, const T *xg, bool xlane, 
 #pragma unroll
             for (int i = 0; i < NP; ++i) a[i] = -a[i];
         }
-        const T in = xlane ? xg[slot] : T(0);
-        if constexpr (REV)
-            step_scatter<T, NP>(a, h, u, in);
-        else
-            h[u] = step_dot<T, NP>(a, h, u, in);
+        const T xv = xmask ? xg[slot] : T(0);
+#pragma unroll
+        for (int q = 0; q < KF; ++q) {
+            const T in = ((xmask >> q) & 1u) ? xv : T(0);
+            if constexpr (REV)
+                step_scatter<T, NP>(a, h[q], u, in);
+            else
+                h[q][u] = step_dot<T, NP>(a, h[q], u, in);
+        }
+    }
+}
+
+// Filters per phase-A lane: two at orders 8..16, where one 16-byte broadcast
+// row load per step otherwise feeds a single recurrence and the shared-memory
+// wavefronts (one per coefficient and warp) bound the phase.
+__host__ __device__ constexpr int filters_per_lane(int NP) { return NP >= 8 && NP <= 16 ? 2 : 1; }
+
+// Stores the state of filter f of a chunk into an affine map laid out as NP
+// rows of stride rs then z: basis filter f < N is column f of P, the
+// zero-state filter f == N is z; f > N (an idle filter slot) stores nothing.
+template <typename T, int NP, bool REV>
+__device__ __forceinline__ void put_map_column(T *M, int rs, const T (&h)[NP], int f, int N) {
+    if (f > N) return;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+        if (i < N) {
+            const T v = h[state_slot<REV, NP>(i)];
+            if (f < N)
+                M[i * rs + f] = v;
+            else
+                M[NP * rs + i] = v;
+        }
     }
 }
 
@@ -534,8 +563,10 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
     int Gp = 1;
     while (Gp < G) Gp <<= 1;
 
-    const int grp = tid / (N + 1);
-    const int kk = tid - grp * (N + 1);
+    constexpr int KF = filters_per_lane(NP);
+    const int TPC = (N + KF) / KF;  // phase-A lanes per chunk: N+1 filters, KF per lane
+    const int grp = tid / TPC;
+    const int kk = tid - grp * TPC;  // lane kk runs filters kk*KF .. kk*KF+KF-1
     const int nwin = L / W;  // windows per pass (phase D: the same count of WD-step windows)
     const int64_t nbatches = p.roff ? p.bb[p.nsig] : p.nbatches;
     Sig *sgs = reinterpret_cast<Sig *>(misc + 1);
@@ -601,10 +632,15 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
             for (int e = tid; e < 2 * G * GSA; e += THREADS)
                 if ((e % GSA) % NP >= N) Abuf[e] = T(0);
         const bool active = grp < Gb;
-        const bool xlane = (kk == N);
-        T h[NP];
+        unsigned xmask = 0;
+        T h[KF][NP];
 #pragma unroll
-        for (int j = 0; j < NP; ++j) h[j] = (active && !xlane && j == state_slot<REV, NP>(kk)) ? T(1) : T(0);
+        for (int q = 0; q < KF; ++q) {
+            const int f = kk * KF + q;
+            if (f == N) xmask |= 1u << q;
+#pragma unroll
+            for (int j = 0; j < NP; ++j) h[q][j] = (active && f < N && j == state_slot<REV, NP>(f)) ? T(1) : T(0);
+        }
 
         LA::load(p, sg, tb, Gb, L, 0, Abuf, ibuf, nullptr, false);
         cp_async_commit();
@@ -618,24 +654,17 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
             __syncthreads();
             if (active) {
                 if (w == nwin / 2) {
-                    // the state after the first half of the chunk: column kk of
-                    // the half map (basis lanes) or its z (zero-state lane)
-                    T *Hg = hmap + (size_t)grp * HME;
+                    // the state after the first half of the chunk: the lane's
+                    // columns of the half map (or its z)
 #pragma unroll
-                    for (int i = 0; i < NP; ++i) {
-                        if (i < N) {
-                            const T v = h[state_slot<REV, NP>(i)];
-                            if (!xlane)
-                                Hg[i * NP + kk] = v;
-                            else
-                                Hg[NP * NP + i] = v;
-                        }
-                    }
+                    for (int q = 0; q < KF; ++q)
+                        put_map_column<T, NP, REV>(hmap + (size_t)grp * HME, NP, h[q], kk * KF + q, N);
                 }
                 const T *Ag = Abuf + (size_t)s * G * GSA + (size_t)grp * GSA;
                 const T *xg = ibuf + (size_t)s * G * W + (size_t)grp * W;
 #pragma unroll 1
-                for (int blk = 0; blk < W / NP; ++blk) map_steps<T, NP, REV, NEG, W, 0, NP>(Ag, xg, xlane, blk * NP, h);
+                for (int blk = 0; blk < W / NP; ++blk)
+                    map_steps<T, NP, KF, REV, NEG, W, 0, NP>(Ag, xg, xmask, blk * NP, h);
             }
             __syncthreads();
         }
@@ -648,17 +677,8 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
         for (int e = tid; e < Gp * MS; e += THREADS) maps[e] = T(0);
         __syncthreads();
         if (active) {
-            T *Mg = maps + (size_t)grp * MS;
 #pragma unroll
-            for (int i = 0; i < NP; ++i) {
-                if (i < N) {
-                    const T v = h[state_slot<REV, NP>(i)];
-                    if (!xlane)
-                        Mg[i * RS + kk] = v;
-                    else
-                        Mg[NP * RS + i] = v;
-                }
-            }
+            for (int q = 0; q < KF; ++q) put_map_column<T, NP, REV>(maps + (size_t)grp * MS, RS, h[q], kk * KF + q, N);
         }
         for (int e = tid; e < (Gp - Gb) * N; e += THREADS) {
             const int g = Gb + e / N;
@@ -891,11 +911,11 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                     double v = (double)Hg[NP * NP + i];
 #pragma unroll
                     for (int k = 0; k < NP; ++k) v = fma((double)Hg[i * NP + k], sg[k], v);
-                    h[state_slot<REV, NP>(i)] = i < N ? (T)v : T(0);
+                    h[0][state_slot<REV, NP>(i)] = i < N ? (T)v : T(0);
                 }
             } else {
 #pragma unroll
-                for (int i = 0; i < NP; ++i) h[state_slot<REV, NP>(i)] = (fix && i < N) ? (T)sg[i] : T(0);
+                for (int i = 0; i < NP; ++i) h[0][state_slot<REV, NP>(i)] = (fix && i < N) ? (T)sg[i] : T(0);
             }
         }
         const bool ti = REV && p.gA && p.as_t == 0;
@@ -921,14 +941,14 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                 T *og = obuf + (size_t)tid * WD;
                 if constexpr (WD % NP == 0) {
 #pragma unroll 1
-                    for (int blk = 0; blk < WD / NP; ++blk) fix_steps<T, NP, REV, NEG, WD, 0, NP>(Ag, xg, og, blk * NP, h);
+                    for (int blk = 0; blk < WD / NP; ++blk) fix_steps<T, NP, REV, NEG, WD, 0, NP>(Ag, xg, og, blk * NP, h[0]);
                 } else {
                     // NP == 2*WD: the ring advances by half a turn per window
                     static_assert(NP == 2 * WD, "window/order mismatch");
                     if (w & 1)
-                        fix_steps<T, NP, REV, NEG, WD, WD, WD>(Ag, xg, og, 0, h);
+                        fix_steps<T, NP, REV, NEG, WD, WD, WD>(Ag, xg, og, 0, h[0]);
                     else
-                        fix_steps<T, NP, REV, NEG, WD, 0, WD>(Ag, xg, og, 0, h);
+                        fix_steps<T, NP, REV, NEG, WD, 0, WD>(Ag, xg, og, 0, h[0]);
                 }
             }
             __syncthreads();
@@ -995,7 +1015,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
                 const int64_t k = npad + i;
-                if (i < N && k < N) p.gzi[sg.zo + k] = h[state_slot<REV, NP>(i)];
+                if (i < N && k < N) p.gzi[sg.zo + k] = h[0][state_slot<REV, NP>(i)];
             }
         }
     }
@@ -1014,7 +1034,7 @@ inline int64_t default_chunk(int64_t T) { return T < 65536 ? kChunkLen / 2 : (T 
 std::atomic<int64_t> g_chunk_target{0};
 constexpr int kMaxChunksPerBatch = 64;
 
-inline int threads_for(int) { return 256; }  // scan group: one group of N+1 lanes per chunk
+inline int threads_for(int) { return 256; }  // scan group: one group of phase-A lanes per chunk
 inline int window_for(int NP) { return window_steps(NP); }
 
 struct Plan {
@@ -1034,7 +1054,12 @@ inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N, int64_t dflt 
     // long ones fewer look-back hops per sample
     const int64_t target = want > 0 ? want : (dflt > 0 ? dflt : default_chunk(T));
     pl.L = (int)(2 * W * ((target + 2 * W - 1) / (2 * W)));  // an even number of windows: halves split on one
+    // chunks per batch: one group of phase-A lanes per chunk; with two filters
+    // per lane at most 16 (a power-of-two tree; larger batches measured slower)
+    const int KF = filters_per_lane(pl.NP);
     int G = (int)(threads_for(pl.NP) / (N + 1));
+    const int Gk = (int)(threads_for(pl.NP) / ((N + KF) / KF));
+    if (Gk > G) G = Gk < 16 ? Gk : (G > 16 ? G : 16);
     if (G > kMaxChunksPerBatch) G = kMaxChunksPerBatch;
     const int ctas = ctas_per_sm(pl.NP, (int)esz);
     const size_t budget = (size_t)228 * 1024 / ctas - 1024;  // per-SM shared memory less the per-CTA reserve
