@@ -317,8 +317,11 @@ struct Loader {
         }
     }
 
-    // Vector path: all threads, one 16-byte cp.async per vector of a chunk's
-    // rows, inputs and lagged outputs.  The caller commits the group.
+    // Vector path: one warp per chunk (chunks warp, warp + 8, ...), so the
+    // row range of a chunk's window is computed once per warp; the chunk's
+    // rows are one contiguous run in global and shared memory, lane l moving
+    // vectors l, l+32, ...  Inputs and lagged outputs follow on the low lanes.
+    // The caller commits the group.
     __device__ static void load_vec(const ChunkParams<T> &p, const Sig &sg, int64_t tb, int Gc, int Lc, int w,
                                     T *As, T *xs, T *ys, bool with_y) {
         constexpr int V = 16 / sizeof(T);
@@ -326,46 +329,56 @@ struct Loader {
         constexpr int AV = WC * RV;                  // coefficient vectors per chunk window
         constexpr int XV = WC / V > 0 ? WC / V : 1;  // input vectors
         constexpr int YV = PY / V;                   // lagged-output vectors
-        const int per = AV + (xs ? XV + ((REV && with_y) ? YV : 0) : 0);  // rows only when xs is null
-        const int tid = threadIdx.x;
+        constexpr int NWARP = THREADS / 32;
+        using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+        const int lane = threadIdx.x & 31;
+        const int nyv = (xs && REV && with_y) ? YV : 0;
+        const int nio = xs ? XV + nyv : 0;  // input-side vectors per chunk
         const T *Ab = p.A + sg.ao;
         const T *inb = p.in + sg.xo;
-        for (int e = tid; e < Gc * per; e += THREADS) {
-            const int g = e / per;
-            const int q = e - g * per;
+        const VT zero = {};
+        for (int g = threadIdx.x >> 5; g < Gc; g += NWARP) {
             int64_t row0;
             int lo, hi;
             rows(sg, tb, Lc, g, w, row0, lo, hi);
-            if (q < AV) {
-                const int r = q / RV;
-                T *dst = As + (size_t)g * GS + q * V;
-                if (r >= lo && r < hi) {
-                    cp_async<16>(dst, Ab + row0 * NP + q * V);
-                } else {
+            T *dA = As + (size_t)g * GS;
+            if (lo == 0 && hi == WC) {
+                const T *sA = Ab + row0 * NP;
 #pragma unroll
-                    for (int j = 0; j < V; ++j) dst[j] = T(0);
-                }
-            } else if (q < AV + XV) {
-                const int r = (q - AV) * V;  // lo, hi and r are multiples of V
-                T *dst = xs + (size_t)g * WC + r;
-                if (r >= lo && r < hi) {
-                    cp_async<16>(dst, inb + row0 + r);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < V; ++j) dst[j] = T(0);
+                for (int k = 0; k < (AV + 31) / 32; ++k) {
+                    const int v = lane + 32 * k;
+                    if (AV % 32 == 0 || v < AV) cp_async<16>(dA + v * V, sA + v * V);
                 }
             } else {
-                const int r = (q - AV - XV) * V;
-                T *dst = ys + (size_t)g * PY + r;
-                const int64_t j0 = row0 - NP + r;  // a multiple of V: all or none of the vector is before t = 0
-                if (j0 >= 0) {
-                    cp_async<16>(dst, p.ysave + sg.xo + j0);
+                for (int v = lane; v < AV; v += 32) {
+                    const int r = v / RV;
+                    if (r >= lo && r < hi)
+                        cp_async<16>(dA + v * V, Ab + (row0 + r) * NP + (v - r * RV) * V);
+                    else
+                        *reinterpret_cast<VT *>(dA + v * V) = zero;
+                }
+            }
+            for (int v = lane; v < nio; v += 32) {
+                if (v < XV) {
+                    const int r = v * V;  // lo, hi and r are multiples of V
+                    T *dst = xs + (size_t)g * WC + r;
+                    if (r >= lo && r < hi)
+                        cp_async<16>(dst, inb + row0 + r);
+                    else
+                        *reinterpret_cast<VT *>(dst) = zero;
                 } else {
-                    const T *zib = p.zi ? p.zi + sg.zo : nullptr;
+                    const int r = (v - XV) * V;
+                    T *dst = ys + (size_t)g * PY + r;
+                    const int64_t j0 = row0 - NP + r;  // a multiple of V: all or none of the vector is before t = 0
+                    if (j0 >= 0) {
+                        cp_async<16>(dst, p.ysave + sg.xo + j0);
+                    } else {
+                        const T *zib = p.zi ? p.zi + sg.zo : nullptr;
 #pragma unroll
-                    for (int j = 0; j < V; ++j) {
-                        const int64_t k = -1 - (j0 + j);
-                        dst[j] = (k >= 0 && k < p.N && zib) ? zib[k] : T(0);
+                        for (int j = 0; j < V; ++j) {
+                            const int64_t k = -1 - (j0 + j);
+                            dst[j] = (k >= 0 && k < p.N && zib) ? zib[k] : T(0);
+                        }
                     }
                 }
             }
