@@ -385,58 +385,53 @@ struct Loader {
         }
     }
 
-    // Element path: all threads, one cp.async per element (any stride and
-    // alignment).  The caller commits the group.
+    // Element path (any stride and alignment): one warp per chunk, one
+    // cp.async per element.  The caller commits the group.
     __device__ static void load_elem(const ChunkParams<T> &p, const Sig &sg, int64_t tb, int Gc, int Lc, int w,
                                      T *As, T *xs, T *ys, bool with_y, bool rows_too) {
+        constexpr int NWARP = THREADS / 32;
         const int N = p.N;
-        const int tid = threadIdx.x;
+        const int lane = threadIdx.x & 31;
         const T *Ab = p.A + sg.ao;
         const T *inb = p.in + sg.xo;
-        const int per = WC * N;
-        for (int e = tid; rows_too && e < Gc * per; e += THREADS) {
-            const int g = e / per;
-            const int rem = e - g * per;
-            const int r = rem / N;
-            const int i = rem - r * N;
+        const T *zib = p.zi ? p.zi + sg.zo : nullptr;
+        for (int g = threadIdx.x >> 5; g < Gc; g += NWARP) {
             int64_t row0;
             int lo, hi;
             rows(sg, tb, Lc, g, w, row0, lo, hi);
-            T *dst = As + (size_t)g * GS + r * NP + i;
-            if (r >= lo && r < hi)
-                cp_async<sizeof(T)>(dst, Ab + (row0 + r) * p.as_t + i);
-            else
-                *dst = T(0);
-        }
-        // inputs (x forward, grad_y backward), slot r <-> index row0 + r
-        for (int e = tid; e < Gc * WC; e += THREADS) {
-            const int g = e / WC;
-            const int r = e - g * WC;
-            int64_t row0;
-            int lo, hi;
-            rows(sg, tb, Lc, g, w, row0, lo, hi);
-            if (r >= lo && r < hi)
-                cp_async<sizeof(T)>(xs + e, inb + row0 + r);
-            else
-                xs[e] = T(0);
-        }
-        if (REV && with_y) {
-            const T *yb = p.ysave + sg.xo;
-            const T *zib = p.zi ? p.zi + sg.zo : nullptr;
-            for (int e = tid; e < Gc * PY; e += THREADS) {
-                const int g = e / PY;
-                const int r = e - g * PY;
-                int64_t row0;
-                int lo, hi;
-                rows(sg, tb, Lc, g, w, row0, lo, hi);
-                const int64_t j = row0 - NP + r;
-                T *dst = ys + e;
-                if (j >= 0)  // j < top <= T
-                    cp_async<sizeof(T)>(dst, yb + j);
-                else if (-1 - j < N && zib)
-                    *dst = zib[-1 - j];
+            if (rows_too) {
+                // element e of the window is tap e % NP of row e / NP (a
+                // compile-time divisor); taps N..NP-1 keep the zeros filled per batch
+                T *dA = As + (size_t)g * GS;
+                for (int e = lane; e < WC * NP; e += 32) {
+                    const int r = e / NP;
+                    const int i = e - r * NP;
+                    if (i >= N) continue;
+                    if (r >= lo && r < hi)
+                        cp_async<sizeof(T)>(dA + e, Ab + (row0 + r) * p.as_t + i);
+                    else
+                        dA[e] = T(0);
+                }
+            }
+            // inputs (x forward, grad_y backward), slot r <-> index row0 + r
+            for (int r = lane; r < WC; r += 32) {
+                T *dst = xs + (size_t)g * WC + r;
+                if (r >= lo && r < hi)
+                    cp_async<sizeof(T)>(dst, inb + row0 + r);
                 else
                     *dst = T(0);
+            }
+            if (REV && with_y) {
+                for (int r = lane; r < PY; r += 32) {
+                    const int64_t j = row0 - NP + r;
+                    T *dst = ys + (size_t)g * PY + r;
+                    if (j >= 0)  // j < top <= T
+                        cp_async<sizeof(T)>(dst, p.ysave + sg.xo + j);
+                    else if (-1 - j < N && zib)
+                        *dst = zib[-1 - j];
+                    else
+                        *dst = T(0);
+                }
             }
         }
     }
@@ -978,43 +973,43 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                     p.gzi[sg.zo + (pos - sg.T)] = obuf[e];
                 }
             }
-            if (REV && p.gA) {
-                // row t = top-WD+rr of half-chunk g: grad_x[t] = obuf[g][WD-1-rr],
-                // y[t-1-i] = ys[g][rr+NP-1-i]
+            if (REV && p.gA && !ti) {
+                // one warp per half-chunk: row t = top-WD+rr has grad_x[t] =
+                // obuf[g][WD-1-rr] and y[t-1-i] = ys[g][rr+NP-1-i]
                 const T sgn = NEG ? T(1) : T(-1);
-                if (!ti && gA_vec) {
-                    // rows [top-WD, top) are contiguous in grad_A: one 16-byte
-                    // vector of taps per thread and row
-                    constexpr int QR = NP / V > 0 ? NP / V : 1;  // vectors per row (gA_vec: NP % V == 0)
-                    constexpr int QPC = WD * QR;                 // vectors per half-chunk window
-                    using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-                    for (int e = tid; e < Gd * QPC; e += THREADS) {
-                        const int g = e / QPC;
-                        const int v = e - g * QPC;
-                        const int rr = v / QR;
-                        const int i0 = (v - rr * QR) * V;
-                        const int64_t top = sg.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
-                        const int64_t t = top - WD + rr;
-                        if (t < 0) continue;
-                        const T gx = sgn * obuf[g * WD + (WD - 1 - rr)];
-                        const T *yq = ys + g * PYD + rr + NP - 1 - i0;
-                        VT o;
-                        T *ov = reinterpret_cast<T *>(&o);
+                for (int g = tid >> 5; g < Gd; g += THREADS / 32) {
+                    const int64_t top = sg.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
+                    const T *og = obuf + g * WD + (WD - 1);
+                    const T *yg = ys + g * PYD + NP - 1;
+                    if (gA_vec) {
+                        // rows [top-WD, top) are one contiguous run of grad_A:
+                        // vector v of the run holds taps i0.. of row rr
+                        constexpr int QR = NP / V > 0 ? NP / V : 1;  // vectors per row (gA_vec: NP % V == 0)
+                        constexpr int QPC = WD * QR;                 // vectors per half-chunk window
+                        using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+                        const int64_t r0 = sg.xo + top - WD;  // row of slot 0; rows with t < 0 are skipped
 #pragma unroll
-                        for (int j = 0; j < V; ++j) ov[j] = gx * yq[-j];
-                        *reinterpret_cast<VT *>(p.gA + (sg.xo + t) * NP + i0) = o;
-                    }
-                } else if (!ti) {
-                    const int per = WD * N;
-                    for (int e = tid; e < Gd * per; e += THREADS) {
-                        const int g = e / per;
-                        const int remg = e - g * per;
-                        const int rr = remg / N;
-                        const int i = remg - rr * N;
-                        const int64_t top = sg.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
-                        const int64_t t = top - WD + rr;
-                        if (t < 0) continue;
-                        p.gA[(sg.xo + t) * N + i] = sgn * obuf[g * WD + (WD - 1 - rr)] * ys[g * PYD + rr + NP - 1 - i];
+                        for (int k = 0; k < (QPC + 31) / 32; ++k) {
+                            const int v = lane + 32 * k;
+                            const int rr = v / QR;
+                            if ((QPC % 32 != 0 && v >= QPC) || top - WD + rr < 0) continue;
+                            const int i0 = (v - rr * QR) * V;
+                            const T gx = sgn * og[-rr];
+                            const T *yq = yg + rr - i0;
+                            VT o;
+                            T *ov = reinterpret_cast<T *>(&o);
+#pragma unroll
+                            for (int j = 0; j < V; ++j) ov[j] = gx * yq[-j];
+                            *reinterpret_cast<VT *>(p.gA + (r0 + rr) * NP + i0) = o;
+                        }
+                    } else {
+                        for (int e = lane; e < WD * N; e += 32) {
+                            const int rr = e / N;
+                            const int i = e - rr * N;
+                            const int64_t t = top - WD + rr;
+                            if (t < 0) continue;
+                            p.gA[(sg.xo + t) * N + i] = sgn * og[-rr] * yg[rr - i];
+                        }
                     }
                 }
             }
