@@ -139,10 +139,33 @@ def bytes_per_sample(N: int, time_invariant: bool):
 
 
 # --------------------------------------------------------------------------- workloads
-def load_workload(cfg: str, device, seed: int = 0, B=None, T=None):
-    from torchlpc_b200.synth import make_workload
+def _synth():
+    """The workload generator, loaded from its file so that importing it does
+    not import the torchlpc_b200 package (and its native libraries): the
+    reference arm uses it too."""
+    name = "_lpc_b200_synth"
+    if name in sys.modules:
+        return sys.modules[name]
+    import importlib.util
 
-    return make_workload(cfg, seed=seed, device=device, B=B, T=T)
+    spec = importlib.util.spec_from_file_location(name, ROOT / "torchlpc_b200" / "synth.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_workload(cfg: str, device, seed: int = 0, B=None, T=None):
+    return _synth().make_workload(cfg, seed=seed, device=device, B=B, T=T)
+
+
+def config_of(args, w, ws: int) -> dict:
+    """The workload description both arms print (same keys, same values)."""
+    A = w["A"]
+    return {"workload": f"{args.config}: {w['workload'].note}", "B": w["B"], "T": w["T"], "N": w["N"],
+            "samples_per_step": samples_of(w),
+            "l2": "inputs larger than L2 (coefficients alone %.0f MiB)" % (A.numel() * A.element_size() / 2 ** 20),
+            "parallelism": f"replicas x{ws} (independent signals, no collective)"}
 
 
 def samples_of(w) -> int:
@@ -225,35 +248,55 @@ def kernel_times(tl, w, x, A, zi, gy, steps, device):
     return tf, tb
 
 
-def accuracy(tl, w, x, A, zi, gy, algo):
-    """Normwise max|out - ref| / max|ref| of y, zf and the three gradients of
-    the float32 path against the float64 sequential kernel on the same
-    (float32-rounded) inputs."""
-    def run(dt, al):
-        tl.set_algo(al)
-        xx = x.detach().to(dt).requires_grad_(True)
-        AA = A.detach().to(dt).requires_grad_(True)
-        zz = zi.detach().to(dt).requires_grad_(True)
-        if w["workload"].ragged:
-            y = tl.sample_wise_lpc_ragged(xx, AA, w["offsets_dev"], zz)
-            zf = None
-        else:
-            y, zf = tl.sample_wise_lpc(xx, coeff_arg(w, AA), zz, return_zf=True)
-        y.backward(gy.to(dt))
-        return {"y": y.detach(), "zf": None if zf is None else zf.detach(), "gx": xx.grad,
-                "gA": AA.grad, "gzi": zz.grad}
+def oracle_errors(tl, w, x, A, zi, gy, max_signals=None):
+    """Normwise max|out - oracle| / max|oracle| of y, zf and the three
+    gradients of the timed float32 path (one untimed fwd+bwd through the public
+    API) against the FP64 sequential oracle (oracle/lpc_oracle.c, the checker)
+    on the same float32 inputs.  Dense workloads compare every signal, or the
+    first ``max_signals``; the ragged workload compares its 32 shortest and 32
+    longest signals out of the full launch."""
+    import numpy as np
 
-    o32 = run(torch.float32, algo)
-    o64 = run(torch.float64, "plain")
-    tl.set_algo(algo)
-    out = {}
-    for k in o32:
-        if o32[k] is None:
-            continue
-        ref = o64[k]
-        den = ref.abs().max().item()
-        out[k] = (o32[k].double() - ref).abs().max().item() / (den if den > 0 else 1.0)
-    return out
+    from oracle import lpc_oracle as O
+
+    xx = x.detach().clone().requires_grad_(True)
+    AA = A.detach().clone().requires_grad_(True)
+    zz = zi.detach().clone().requires_grad_(True)
+    got = {}
+    if w["workload"].ragged:
+        y = tl.sample_wise_lpc_ragged(xx, AA, w["offsets_dev"], zz)
+        y.backward(gy)
+        torch.cuda.synchronize()
+        off = w["offsets"].cpu()
+        lens = (off[1:] - off[:-1]).numpy()
+        order = np.argsort(lens, kind="stable")
+        pick = np.concatenate([order[:32], order[-32:]])
+        rows = torch.from_numpy(np.concatenate([np.arange(int(off[b]), int(off[b + 1])) for b in pick])).to(x.device)
+        sub = np.zeros(len(pick) + 1, np.int64)
+        sub[1:] = np.cumsum(lens[pick])
+        sig = torch.from_numpy(pick).to(x.device)
+        xs, As, gs, zs = x.detach()[rows], A.detach()[rows], gy[rows], zi.detach()[sig]
+        yo = O.lpc_forward_ragged(xs, As, zs, sub)
+        gxo, gAo, gzio = O.lpc_backward_ragged(gs, As, zs, yo, sub)
+        ref = {"y": yo, "gx": gxo, "gA": gAo, "gzi": gzio}
+        got = {"y": y.detach()[rows], "gx": xx.grad[rows], "gA": AA.grad[rows], "gzi": zz.grad[sig]}
+        what = f"{len(pick)} of {w['B']} ragged signals (32 shortest, 32 longest) from the full launch"
+    else:
+        y, zf = tl.sample_wise_lpc(xx, coeff_arg(w, AA), zz, return_zf=True)
+        y.backward(gy)
+        torch.cuda.synchronize()
+        nb = w["B"] if max_signals is None else min(w["B"], max_signals)
+        s = slice(0, nb)
+        yo = O.lpc_forward(x.detach()[s], A.detach()[s], zi.detach()[s])
+        gxo, gAo, gzio = O.lpc_backward(gy[s], A.detach()[s], zi.detach()[s], yo)
+        N = w["N"]
+        ref = {"y": yo, "zf": yo[:, -N:][:, ::-1], "gx": gxo, "gA": gAo, "gzi": gzio}
+        got = {"y": y.detach()[s], "zf": zf.detach()[s], "gx": xx.grad[s], "gA": AA.grad[s], "gzi": zz.grad[s]}
+        what = f"{nb} of {w['B']} signals, full length"
+    errs = {k: O.normwise_err(got[k], ref[k]) for k in ref}
+    tol = 1e-4
+    return {**errs, "max": max(errs.values()), "tolerance": tol, "within": max(errs.values()) <= tol,
+            "oracle": "FP64 sequential C restatement (oracle/lpc_oracle.c)", "compared": what}
 
 
 def e2e_time(tl, w, x_dev, A_dev, zi_dev, gy_dev, steps, warmup, device):
@@ -396,8 +439,9 @@ def run_reference(args):
     if ref is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
-    device = "cuda" if torch.cuda.is_available() else "cpu"
-    w = load_workload(args.config, device, B=args.B, T=args.T)
+    # inputs are generated on the host: this arm runs no GPU work and loads
+    # none of this repository's native libraries
+    w = load_workload(args.config, "cpu", B=args.B, T=args.T)
     once, nsamp, desc = reference_calls(ref, w)
     for _ in range(max(1, args.warmup)):
         once()
@@ -414,7 +458,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {w['workload'].note}", "sample": desc},
+        "config": config_of(args, w, ws),
         "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "reference",
                          "sample": f"{desc}; reference torchlpc CPU operator (scan_cpu.cpp, OpenMP) + "
                                    f"its autograd backward, fp32"},
@@ -445,6 +489,8 @@ def other_configs(tl, headline: str, device) -> dict:
             tf, tb = kernel_times(tl, w, x, A, zi, gy, 3 if algo == "plain" else 10, device)
             entry[algo] = {"GS_per_s": S / ((tf + tb) * 1e-3) / 1e9, "fwd_ms": tf, "bwd_ms": tb}
         tl.set_algo("auto")
+        entry["max_rel_err_vs_fp64"] = oracle_errors(tl, w, x, A, zi, gy,
+                                                     max_signals=256 if w["workload"].time_invariant else None)
         out[cfg] = entry
         del w, x, A, zi, gy
         torch.cuda.empty_cache()
@@ -487,11 +533,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded; x, g ~ N(0,1); per-frame pole pairs interpolated per sample)",
-            "config": {"workload": f"{args.config}: {wl.note}", "B": w["B"], "T": w["T"], "N": w["N"],
-                       "samples_per_step": S, "algo": args.algo,
-                       "l2": "inputs larger than L2 (coefficients alone %.0f MiB)" % (
-                           A.numel() * A.element_size() / 2 ** 20),
-                       "parallelism": f"replicas x{ws} (independent signals, no collective)"},
+            "config": config_of(args, w, ws), "algo": args.algo,
             "gpu_launches": launches_per_step * args.steps}
     if clocks:
         line["clocks"] = clocks
@@ -518,7 +560,7 @@ def run_ours(args):
             tl.set_algo(args.algo)
             line["plain"] = {"value": S / (msp * 1e-3), "ms_per_step": msp,
                              "speedup": msp / ms}
-        line["max_rel_err_vs_fp64"] = accuracy(tl, w, x, A, zi, gy, args.algo)
+        line["max_rel_err_vs_fp64"] = oracle_errors(tl, w, x, A, zi, gy)
         if not args.no_extras and ws == 1:
             line["other_configs"] = other_configs(tl, args.config, device)
             tl.set_algo(args.algo)
