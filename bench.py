@@ -226,9 +226,10 @@ def time_loop(fn, steps, warmup, device):
     return s.elapsed_time(e) / steps  # ms per step
 
 
-def kernel_times(tl, w, x, A, zi, gy, steps, device):
+def kernel_times(tl, w, x, A, zi, gy, steps, device, ckpt=False):
     """Average device time of the forward and the fused backward operator
-    (CUDA events on the launching stream)."""
+    (CUDA events on the launching stream); ``ckpt``: the boundary-state
+    checkpointed pair the public API runs for long signals."""
     from torchlpc_b200 import _ops
 
     Aa = coeff_arg(w, A).detach()
@@ -239,6 +240,11 @@ def kernel_times(tl, w, x, A, zi, gy, steps, device):
             fwd = lambda: _ops.lpc_ragged(x.detach(), A.detach(), w["offsets_dev"], zi.detach())
             y = fwd()
             bwd = lambda: _ops.lpc_backward_ragged(gy, A.detach(), w["offsets_dev"], zi.detach(), y, True, True)
+        elif ckpt:
+            L = _ops.checkpoint_chunk(w["T"], w["N"], x.dtype)
+            fwd = lambda: _ops.lpc_checkpointed(x.detach(), Aa, zi.detach(), L)
+            _, states = fwd()
+            bwd = lambda: _ops.lpc_backward_checkpointed(gy, Aa, zi.detach(), x.detach(), states, L, True, True)
         else:
             fwd = lambda: _ops.lpc(x.detach(), Aa, zi.detach())
             y = fwd()
@@ -299,34 +305,58 @@ def oracle_errors(tl, w, x, A, zi, gy, max_signals=None):
             "oracle": "FP64 sequential C restatement (oracle/lpc_oracle.c)", "compared": what}
 
 
-def e2e_time(tl, w, x_dev, A_dev, zi_dev, gy_dev, steps, warmup, device):
+def e2e_time(tl, w, x_dev, A_dev, zi_dev, gy_dev, steps, warmup, device, slices=8):
     """The same step through the public API with HOST inputs: every step copies
-    x, A, zi, grad_y from pinned host memory and reads y and the three
-    gradients back into pinned host memory."""
+    x, A, zi and grad_y from pinned host memory and reads y and the three
+    gradients back into pinned host memory.  The batch is cut into ``slices``
+    groups of whole signals, filtered independently and pipelined over two
+    CUDA streams (host-to-device copy, fwd+bwd, device-to-host copy), so that
+    the copies of one group overlap the compute and the opposite copy
+    direction of its neighbours; every copy is one cudaMemcpyAsync of a
+    contiguous range.  Dense workloads only (ragged: one group)."""
     hx, hA, hz, hg = (t.detach().cpu().pin_memory() for t in (x_dev, A_dev, zi_dev, gy_dev))
     outs = {k: torch.empty(s, dtype=x_dev.dtype).pin_memory()
             for k, s in (("y", x_dev.shape), ("gx", x_dev.shape), ("gA", A_dev.shape), ("gzi", zi_dev.shape))}
     ragged = w["workload"].ragged
+    B = hx.shape[0]
+    k = 1 if ragged else max(1, min(slices, B))
+    bounds = [(i * B // k, (i + 1) * B // k) for i in range(k)]
+    streams = [torch.cuda.Stream(device) for _ in range(2)]
+    main = torch.cuda.current_stream(device)
+
+    def one(lo, hi, st):
+        with torch.cuda.stream(st):
+            sl = slice(lo, hi)
+            if ragged:
+                x, A, zi, gy = (t.to(device, non_blocking=True) for t in (hx, hA, hz, hg))
+            else:
+                x, A, zi, gy = (t[sl].to(device, non_blocking=True) for t in (hx, hA, hz, hg))
+            x.requires_grad_(True)
+            A.requires_grad_(True)
+            zi.requires_grad_(True)
+            if ragged:
+                y = tl.sample_wise_lpc_ragged(x, A, w["offsets_dev"], zi)
+            else:
+                y = tl.sample_wise_lpc(x, coeff_arg(w, A), zi)
+            y.backward(gy)
+            dst = (lambda t: outs[t]) if ragged else (lambda t: outs[t][sl])
+            dst("y").copy_(y.detach(), non_blocking=True)
+            dst("gx").copy_(x.grad, non_blocking=True)
+            dst("gA").copy_(A.grad, non_blocking=True)
+            dst("gzi").copy_(zi.grad, non_blocking=True)
 
     def step():
-        x = hx.to(device, non_blocking=True).requires_grad_(True)
-        A = hA.to(device, non_blocking=True).requires_grad_(True)
-        zi = hz.to(device, non_blocking=True).requires_grad_(True)
-        gy = hg.to(device, non_blocking=True)
-        if ragged:
-            y = tl.sample_wise_lpc_ragged(x, A, w["offsets_dev"], zi)
-        else:
-            y = tl.sample_wise_lpc(x, coeff_arg(w, A), zi)
-        y.backward(gy)
-        outs["y"].copy_(y.detach(), non_blocking=True)
-        outs["gx"].copy_(x.grad, non_blocking=True)
-        outs["gA"].copy_(A.grad, non_blocking=True)
-        outs["gzi"].copy_(zi.grad, non_blocking=True)
+        for st in streams:
+            st.wait_stream(main)
+        for i, (lo, hi) in enumerate(bounds):
+            one(lo, hi, streams[i % 2])
+        for st in streams:
+            main.wait_stream(st)
 
     ms = time_loop(step, steps, warmup, device)
     h2d = sum(t.numel() * t.element_size() for t in (hx, hA, hz, hg))
     d2h = sum(t.numel() * t.element_size() for t in outs.values())
-    return ms, h2d, d2h
+    return ms, h2d, d2h, k
 
 
 def traffic_from_profiles(cfg: str, kernel: str):
@@ -520,6 +550,9 @@ def run_ours(args):
     gy = w["gy"]
     step = make_step(tl, w, x, A, zi, gy)
 
+    y0 = step()
+    ckpt = y0.grad_fn is not None and "LPCBoundary" in type(y0.grad_fn).__name__
+    del y0
     launches_per_step = count_kernels(step)
     sampler = ClockSampler(torch.cuda.current_device()) if rk == 0 else None
     if sampler:
@@ -534,13 +567,16 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded; x, g ~ N(0,1); per-frame pole pairs interpolated per sample)",
             "config": config_of(args, w, ws), "algo": args.algo,
-            "gpu_launches": launches_per_step * args.steps}
+            "gpu_launches": launches_per_step * args.steps,
+            "checkpointing": ("boundary states: the forward kernel keeps every half-chunk's entry state instead "
+                              "of y; the backward recomputes y from them and x (one exact pass over independent "
+                              "half-chunks) before the fused backward kernel" if ckpt else "off (y saved)")}
     if clocks:
         line["clocks"] = clocks
 
     if rk == 0:
         # roofline of the dominant kernel (forward or fused backward operator)
-        tf, tb = kernel_times(tl, w, x, A, zi, gy, max(5, args.steps // 2), device)
+        tf, tb = kernel_times(tl, w, x, A, zi, gy, max(5, args.steps // 2), device, ckpt=ckpt)
         peak, peak_kind = measured_peaks()
         bf, bb = bytes_per_sample(w["N"], wl.time_invariant)
         kern, t_k, b_k = ("backward", tb, bb) if tb >= tf else ("forward", tf, bf)
@@ -553,6 +589,15 @@ def run_ours(args):
         step_bytes = S * (bf + bb)
         line["hbm_frac_fwd_bwd"] = step_bytes / (ms * 1e-3) / 1e9 / peak
         line["kernel_ms"] = {"forward": tf, "backward": tb}
+        if ckpt:
+            # the same step keeping y for the backward instead of the states
+            old = tl.get_checkpointing()
+            tl.set_checkpointing("off")
+            mss = time_loop(step, args.steps, 3, device)
+            tsf, tsb = kernel_times(tl, w, x, A, zi, gy, max(5, args.steps // 2), device, ckpt=False)
+            tl.set_checkpointing(old)
+            line["saved_y"] = {"value": S / (mss * 1e-3), "ms_per_step": mss,
+                               "kernel_ms": {"forward": tsf, "backward": tsb}}
         # scan vs plain on the same GPU
         if args.algo != "plain" and "chunked" in tl.available_algos():
             tl.set_algo("plain")
@@ -565,9 +610,10 @@ def run_ours(args):
             line["other_configs"] = other_configs(tl, args.config, device)
             tl.set_algo(args.algo)
         if not args.no_e2e:
-            ems, h2d, d2h = e2e_time(tl, w, x, A, zi, gy, max(3, args.steps // 4), 2, device)
+            ems, h2d, d2h, nsl = e2e_time(tl, w, x, A, zi, gy, max(3, args.steps // 4), 3, device)
             line["e2e"] = {"value": S / (ems * 1e-3), "unit": "samples/s", "ms_per_step": ems,
-                           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+                           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                           "pipeline": f"{nsl} groups of signals over 2 CUDA streams (copies overlap compute)"}
         if ws == 1 and not args.no_cpu_baseline:
             ref, why = reference_module()
             if ref is not None:

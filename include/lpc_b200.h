@@ -101,6 +101,52 @@ int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A,
                       size_t workspace_bytes, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Boundary-state checkpointing (chunked scan, time-varying coefficients).
+ * Replaces what LPC.setup_context saves for the backward
+ * (torchlpc/core.py:179-184 keeps (A, zi, y)): the checkpointed forward
+ * writes y and, into `states`, the exact N-sample state entering every
+ * half-chunk of the scan; the checkpointed backward then needs x and those
+ * states instead of y: it recomputes y inside its workspace with one exact
+ * pass over independent half-chunks (no maps, no look-back), then runs the
+ * fused backward on it.  The gradients are those of lpc_b200_backward.
+ * y is therefore not held between the two calls; the backward's workspace
+ * holds a B*T copy while it runs.
+ * lpc_b200_checkpoint_chunk gives the chunk length the current setting picks
+ * for signals of T samples; pass the same chunk_len to both calls (it fixes
+ * how the signal is cut, so the chunk-length setting may change in between).
+ * lpc_b200_checkpoint_elems gives the number of elements of `states` (dtype
+ * as x), about 2*B*T*N/chunk_len.  a_stride_t must be at least N
+ * (time-invariant coefficients return LPC_ERR_UNSUPPORTED: their backward
+ * runs the time-invariant scan on y); orders above 32 return
+ * LPC_ERR_UNSUPPORTED.
+ * ------------------------------------------------------------------------- */
+int64_t lpc_b200_checkpoint_chunk(int dtype, int64_t T, int64_t N);
+
+int64_t lpc_b200_checkpoint_elems(int dtype, int64_t B, int64_t T, int64_t N,
+                                  int64_t chunk_len);
+
+size_t lpc_b200_forward_checkpointed_workspace_size(int dtype, int64_t B, int64_t T,
+                                                    int64_t N, int64_t chunk_len);
+
+int lpc_b200_forward_checkpointed(int dtype, const void *x, const void *A,
+                                  const void *zi, void *y, void *states, int64_t B,
+                                  int64_t T, int64_t N, int64_t a_stride_b,
+                                  int64_t a_stride_t, int64_t chunk_len,
+                                  void *workspace, size_t workspace_bytes,
+                                  void *stream);
+
+size_t lpc_b200_backward_checkpointed_workspace_size(int dtype, int64_t B, int64_t T,
+                                                     int64_t N, int64_t chunk_len);
+
+int lpc_b200_backward_checkpointed(int dtype, const void *grad_y, const void *A,
+                                   const void *zi, const void *x, const void *states,
+                                   void *grad_x, void *grad_A, void *grad_zi,
+                                   int64_t B, int64_t T, int64_t N, int64_t a_stride_b,
+                                   int64_t a_stride_t, int64_t chunk_len,
+                                   void *workspace, size_t workspace_bytes,
+                                   void *stream);
+
+/* ---------------------------------------------------------------------------
  * Forward filter with no workspace argument, for callers that cannot allocate
  * device memory (code that must not call an allocator, such as a real-time
  * audio thread or a host callback, or an FFI binding without a memory
@@ -121,6 +167,14 @@ int lpc_b200_forward_noalloc(int dtype, const void *x, const void *A,
                              int64_t N, int64_t a_stride_b, int64_t a_stride_t,
                              void *stream);
 
+/* Status word of the last lpc_b200_forward_noalloc call on the current device
+ * (the word sits in the library's own scratch array, where
+ * lpc_b200_workspace_status cannot reach it): synchronises `stream` and
+ * copies the word to *status (host memory).  Nonzero means a bounded wait of
+ * that call gave up and its y is invalid; the call itself still returned
+ * LPC_OK, since it returns before the kernel runs.  Allocates nothing. */
+int lpc_b200_noalloc_status(unsigned *status, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Failure detection.  No reference counterpart (the reference kernels have no
  * bounded waits).  The chunked kernels' waits on other CTAs are bounded; when
@@ -135,6 +189,16 @@ int lpc_b200_forward_noalloc(int dtype, const void *x, const void *A,
  * *status when the wait gave up as designed.
  * ------------------------------------------------------------------------- */
 int lpc_b200_workspace_status(const void *workspace, unsigned *status, void *stream);
+
+/* Process-wide error word (no reference counterpart): when set, every chunked
+ * kernel whose status word ends nonzero ORs it into *word when its CTAs
+ * finish, so a caller learns that a call's outputs are invalid without
+ * keeping or reading that call's workspace.  `word` must stay valid and
+ * device-writable for as long as it is set: mapped pinned host memory
+ * (cudaHostAllocMapped; the host then reads it without a CUDA call) or device
+ * memory.  The word is only ever OR-ed into; the caller clears it.  NULL
+ * turns the reporting off (the default). */
+int lpc_b200_set_error_word(unsigned *word);
 
 size_t lpc_b200_selftest_workspace_size(void);
 

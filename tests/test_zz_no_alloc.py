@@ -32,6 +32,7 @@ def lib():
     L.lpc_b200_forward_workspace_size.argtypes = [C.c_int, C.c_int, i64, i64, i64, i64]
     L.lpc_b200_forward_workspace_size.restype = sz
     L.lpc_b200_forward_noalloc.argtypes = [C.c_int, vp, vp, vp, vp, i64, i64, i64, i64, i64, vp]
+    L.lpc_b200_noalloc_status.argtypes = [C.POINTER(C.c_uint), vp]
     return L
 
 
@@ -55,6 +56,36 @@ def test_noalloc_matches_workspace_entry_point_twice(lib):
         torch.cuda.synchronize()
         assert O.normwise_err(y, y_ref) < TOL
         assert O.normwise_err(y, O.lpc_forward(w["x"], w["A"], w["zi"])) < TOL
+
+
+@pytest.mark.parametrize("dtype,code,tol", [(torch.float32, 0, 1e-4), (torch.float64, 1, 1e-10)])
+@pytest.mark.parametrize("with_zi", [True, False])
+@pytest.mark.parametrize("time_invariant", [False, True])
+def test_noalloc_dtypes_initial_conditions_and_strides(lib, dtype, code, tol, with_zi, time_invariant):
+    """float32 and float64, zi given or NULL, dense (B,T,N) coefficients or a
+    stride-0 (B,N) set broadcast over time; two calls in a row, each checked
+    against lpc_b200_forward and the FP64 oracle, and the array's status
+    word read back through lpc_b200_noalloc_status."""
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for seed in (0, 1):
+        cfg = "cfg5" if time_invariant else "cfg3"
+        w = make_workload(cfg, seed=200 + seed, B=3, T=30000 + 7 * seed, dtype=dtype)
+        x, A = w["x"].cuda(), w["A"].cuda()
+        zi = w["zi"].cuda() if with_zi else None
+        B, T = x.shape
+        N = A.shape[-1]
+        sb, stt = (N, 0) if time_invariant else (T * N, N)
+        y_ref = torch.empty_like(x)
+        wsb = lib.lpc_b200_forward_workspace_size(code, 2, B, T, N, stt)
+        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+        assert lib.lpc_b200_forward(code, 2, ptr(x), ptr(A), ptr(zi), ptr(y_ref), B, T, N, sb, stt,
+                                    ptr(ws), wsb, st) == 0
+        y = torch.full_like(x, float("nan"))
+        assert lib.lpc_b200_forward_noalloc(code, ptr(x), ptr(A), ptr(zi), ptr(y), B, T, N, sb, stt, st) == 0
+        status = C.c_uint(7)
+        assert lib.lpc_b200_noalloc_status(C.byref(status), st) == 0 and status.value == 0
+        assert O.normwise_err(y, y_ref) < tol
+        assert O.normwise_err(y, O.lpc_forward(w["x"], w["A"], w["zi"] if with_zi else None)) < tol
 
 
 def test_noalloc_rejects_problems_beyond_its_scratch(lib):

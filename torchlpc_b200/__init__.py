@@ -12,12 +12,15 @@ from typing import Optional, Tuple, Union
 
 import torch
 
-from ._ops import EXTENSION_LOADED, available_algos, get_algo, set_algo
-from .core import LPC, LPCCheckpointed, LPCRagged
+from . import _ops
+from ._ops import EXTENSION_LOADED, available_algos, check_status, get_algo, set_algo
+from .core import LPC, LPCBoundary, LPCCheckpointed, LPCRagged
 from .recurrence import Recurrence
 
 __all__ = ["sample_wise_lpc", "linear_recurrence", "LPC", "Recurrence", "EXTENSION_LOADED",
-           "set_algo", "get_algo", "available_algos", "sample_wise_lpc_ragged", "LPCRagged", "set_checkpoint_segment", "LPCCheckpointed"]
+           "set_algo", "get_algo", "available_algos", "sample_wise_lpc_ragged", "LPCRagged",
+           "set_checkpoint_segment", "LPCCheckpointed", "set_checkpointing", "get_checkpointing", "LPCBoundary",
+           "check_status"]
 
 
 def linear_recurrence(a: torch.Tensor, x: torch.Tensor, zi: Optional[torch.Tensor] = None) -> torch.Tensor:
@@ -65,6 +68,48 @@ def _time_invariant_source(a: torch.Tensor) -> Optional[torch.Tensor]:
 
 
 _CHECKPOINT_SEGMENT = 0
+_CHECKPOINTING = "auto"
+# Signals of at least this many samples keep chunk-boundary states instead of y
+# under the "auto" checkpointing mode.
+CHECKPOINT_MIN_SAMPLES = 1 << 20
+
+
+def set_checkpointing(mode: str) -> None:
+    """Boundary-state checkpointing inside the chunked kernels
+    (``LPCBoundary``): "auto" (default) for signals of at least 2^20 samples,
+    "on" for every signal the chunked scan can take, "off" never.  It applies
+    to time-varying (B,T,N) coefficients of order 2 to 32 under the "auto",
+    "chunked" and "tuned" algorithms, when a gradient is wanted and no
+    forward-mode AD or functorch transform is active; other calls keep y as
+    torchlpc does."""
+    global _CHECKPOINTING
+    assert mode in ("auto", "on", "off"), mode
+    _CHECKPOINTING = mode
+
+
+def get_checkpointing() -> str:
+    return _CHECKPOINTING
+
+
+def _boundary_checkpoint(x: torch.Tensor, A: torch.Tensor, zi: torch.Tensor, T: int, order: int) -> bool:
+    if _CHECKPOINTING == "off" or (_CHECKPOINTING == "auto" and T < CHECKPOINT_MIN_SAMPLES):
+        return False
+    if not (2 <= order <= 32) or A.dim() != 3 or A.stride(1) == 0 or not x.is_cuda:
+        return False
+    if get_algo() == "plain" or x.dtype not in (torch.float32, torch.float64):
+        return False
+    if not torch.is_grad_enabled() or not any(t.requires_grad for t in (x, A, zi)):
+        return False
+    try:
+        from torch._C._functorch import is_functorch_wrapped_tensor
+        from torch.autograd.forward_ad import unpack_dual
+
+        for t in (x, A, zi):
+            if is_functorch_wrapped_tensor(t) or unpack_dual(t).tangent is not None:
+                return False
+    except (ImportError, RuntimeError):
+        return False
+    return True
 
 
 def set_checkpoint_segment(samples: int) -> None:
@@ -112,6 +157,8 @@ def sample_wise_lpc(
         A = src if src is not None else a
         if _CHECKPOINT_SEGMENT and T > _CHECKPOINT_SEGMENT >= order:
             y = LPCCheckpointed.apply(x, A, zi, _CHECKPOINT_SEGMENT)
+        elif _boundary_checkpoint(x, A, zi, T, order):
+            y = LPCBoundary.apply(x, A, zi, _ops.checkpoint_chunk(T, order, x.dtype))
         else:
             y = LPC.apply(x, A, zi)
 

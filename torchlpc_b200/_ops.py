@@ -35,6 +35,8 @@ def _lib():
         lib = ctypes.CDLL(str(Path(__file__).resolve().parent / "liblpc_b200.so"))
         lib.lpc_b200_set_chunk_length.argtypes = [ctypes.c_int64]
         lib.lpc_b200_chunk_length.restype = ctypes.c_int64
+        lib.lpc_b200_checkpoint_chunk.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64]
+        lib.lpc_b200_checkpoint_chunk.restype = ctypes.c_int64
         _LIB = lib
     return _LIB
 
@@ -109,6 +111,37 @@ def scan(impulse, decay, init):
 def scan_backward(grad_out, decay, init, out, need_decay, need_init):
     _require()
     return torch.ops.torchlpc_b200.scan_backward(grad_out, decay, init, out, need_decay, need_init, max(_algo, 0))
+
+
+def checkpoint_chunk(T: int, N: int, dtype) -> int:
+    """Chunk length a checkpointed forward and its backward share (the
+    current chunk-length setting applied to signals of T samples)."""
+    _require()
+    return int(_lib().lpc_b200_checkpoint_chunk(0 if dtype == torch.float32 else 1, int(T), int(N)))
+
+
+def lpc_checkpointed(x, A, zi, chunk):
+    _require()
+    return torch.ops.torchlpc_b200.lpc_checkpointed(x, A, zi, chunk)
+
+
+def lpc_backward_checkpointed(grad_y, A, zi, x, states, chunk, need_A, need_zi):
+    _require()
+    return torch.ops.torchlpc_b200.lpc_backward_checkpointed(grad_y, A, zi, x, states, chunk, need_A, need_zi)
+
+
+def check_status(synchronize: bool = True) -> None:
+    """Raise RuntimeError if a chunked kernel's bounded device-side wait gave
+    up since the last check (its call's outputs are invalid).  Synchronises the
+    current stream first unless ``synchronize`` is False; clears the word.
+    Every operator call also checks it on entry, without synchronising."""
+    _require()
+    w = int(torch.ops.torchlpc_b200.check_status(bool(synchronize)))
+    if w:
+        raise RuntimeError(
+            f"torchlpc_b200: a bounded device-side wait of a chunked kernel gave up (status word {w:#x}; "
+            "1: a predecessor's flag never appeared, 2: inconsistent flags, 8: a ragged signal with a "
+            "negative length); the outputs of that call are invalid")
 
 
 def lpc_ragged(x, A, offsets, zi):

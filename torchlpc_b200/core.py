@@ -124,8 +124,40 @@ class LPCRagged(Function):
         return (gx if needs[0] else None, gA if needs[1] else None, None, gzi if needs[3] else None)
 
 
+class LPCBoundary(Function):
+    """The filter with boundary-state checkpointing in the kernels.
+
+    ``LPCBoundary.apply(x, A, zi, chunk)``: same result as ``LPC.apply(x, A,
+    zi)``.  torchlpc's LPC saves (A, zi, y) for the backward
+    (torchlpc/core.py:179-184); this one saves (x, A, zi) and the N-sample
+    state entering every half of every ``chunk``-sample chunk of the scan,
+    which the checkpointed forward kernel writes beside y (2N values per
+    chunk).  The backward recomputes y from those states with one exact pass
+    over independent half-chunks, then runs the fused backward kernel, so y is
+    not kept alive between forward and backward.  Time-varying (B,T,N)
+    coefficients of order up to 32; not itself differentiable (no
+    forward-mode AD or double backward).
+    """
+
+    @staticmethod
+    def forward(ctx: Any, x: torch.Tensor, A: torch.Tensor, zi: torch.Tensor, chunk: int) -> torch.Tensor:
+        y, states = _ops.lpc_checkpointed(x, A, zi, chunk)
+        ctx.save_for_backward(x, A, zi, states)
+        ctx.chunk = chunk
+        return y
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx: Any, grad_y: torch.Tensor):
+        x, A, zi, states = ctx.saved_tensors
+        needs = ctx.needs_input_grad
+        gx, gA, gzi = _ops.lpc_backward_checkpointed(grad_y, A, zi, x, states, ctx.chunk, bool(needs[1]),
+                                                     bool(needs[2]))
+        return (gx if needs[0] else None, gA if needs[1] else None, gzi if needs[2] else None, None)
+
+
 class LPCCheckpointed(Function):
-    """The filter with boundary-state checkpointing for long signals.
+    """The filter with boundary-state checkpointing for long signals, by segments.
 
     ``LPCCheckpointed.apply(x, A, zi, segment)``: same result as
     ``LPC.apply(x, A, zi)``, but instead of the output y (B,T) it keeps the

@@ -150,6 +150,88 @@ int lpc_b200_backward(int dtype, int algo, const void *grad_y, const void *A, co
                               a_stride_b, a_stride_t, workspace, workspace_bytes, s);
 }
 
+int64_t lpc_b200_checkpoint_chunk(int dtype, int64_t T, int64_t N) {
+    if (!dtype_ok(dtype) || !sizes_ok(1, T, N) || !chunked_supported(N)) return 0;
+    return chunked_checkpoint_chunk(dtype == LPC_F32 ? 4 : 8, T, N);
+}
+
+int64_t lpc_b200_checkpoint_elems(int dtype, int64_t B, int64_t T, int64_t N, int64_t chunk_len) {
+    if (!dtype_ok(dtype) || !sizes_ok(B, T, N)) return 0;
+    return chunked_checkpoint_elems(dtype == LPC_F32 ? 4 : 8, B, T, N, chunk_len);
+}
+
+size_t lpc_b200_forward_checkpointed_workspace_size(int dtype, int64_t B, int64_t T, int64_t N,
+                                                    int64_t chunk_len) {
+    if (!dtype_ok(dtype) || !sizes_ok(B, T, N)) return 0;
+    return chunked_forward_ckpt_workspace(dtype == LPC_F32 ? 4 : 8, B, T, N, chunk_len);
+}
+
+size_t lpc_b200_backward_checkpointed_workspace_size(int dtype, int64_t B, int64_t T, int64_t N,
+                                                     int64_t chunk_len) {
+    if (!dtype_ok(dtype) || !sizes_ok(B, T, N)) return 0;
+    return chunked_backward_ckpt_workspace(dtype == LPC_F32 ? 4 : 8, B, T, N, chunk_len);
+}
+
+namespace {
+int ckpt_check(int dtype, int64_t B, int64_t T, int64_t N, int64_t sb, int64_t st, int64_t chunk_len) {
+    if (!dtype_ok(dtype) || !sizes_ok(B, T, N) || chunk_len <= 0) return LPC_ERR_INVALID_ARGUMENT;
+    if (st < N || sb < 0) return st == 0 ? LPC_ERR_UNSUPPORTED : LPC_ERR_INVALID_ARGUMENT;
+    if (!chunked_supported(N)) return LPC_ERR_UNSUPPORTED;
+    return LPC_OK;
+}
+}  // namespace
+
+int lpc_b200_forward_checkpointed(int dtype, const void *x, const void *A, const void *zi, void *y,
+                                  void *states, int64_t B, int64_t T, int64_t N, int64_t a_stride_b,
+                                  int64_t a_stride_t, int64_t chunk_len, void *workspace,
+                                  size_t workspace_bytes, void *stream) {
+    const int rc = ckpt_check(dtype, B, T, N, a_stride_b, a_stride_t, chunk_len);
+    if (rc != LPC_OK) return rc;
+    if (B == 0 || T == 0) return LPC_OK;
+    if (!x || !A || !y || !states) return LPC_ERR_INVALID_ARGUMENT;
+    const size_t esz = dtype == LPC_F32 ? 4 : 8;
+    if (!workspace || workspace_bytes < chunked_forward_ckpt_workspace(esz, B, T, N, chunk_len))
+        return LPC_ERR_WORKSPACE;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    auto run = [&](auto tag) -> int {
+        using Tt = decltype(tag);
+        FwdArgs<Tt> p{static_cast<const Tt *>(x), static_cast<const Tt *>(A), static_cast<const Tt *>(zi),
+                      static_cast<Tt *>(y), B, T, N, a_stride_b, a_stride_t};
+        return cuda_status(chunked_forward_ckpt<Tt>(p, static_cast<Tt *>(states), chunk_len, workspace,
+                                                    workspace_bytes, s));
+    };
+    return dtype == LPC_F32 ? run(float{}) : run(double{});
+}
+
+int lpc_b200_backward_checkpointed(int dtype, const void *grad_y, const void *A, const void *zi,
+                                   const void *x, const void *states, void *grad_x, void *grad_A,
+                                   void *grad_zi, int64_t B, int64_t T, int64_t N, int64_t a_stride_b,
+                                   int64_t a_stride_t, int64_t chunk_len, void *workspace,
+                                   size_t workspace_bytes, void *stream) {
+    const int rc = ckpt_check(dtype, B, T, N, a_stride_b, a_stride_t, chunk_len);
+    if (rc != LPC_OK) return rc;
+    if (B == 0) return LPC_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t esz = dtype == LPC_F32 ? 4 : 8;
+    if (T == 0) {
+        if (grad_zi) cudaMemsetAsync(grad_zi, 0, (size_t)B * N * esz, s);
+        return cuda_status(cudaGetLastError());
+    }
+    if (!grad_y || !A || !x || !states || !grad_x) return LPC_ERR_INVALID_ARGUMENT;
+    if (!workspace || workspace_bytes < chunked_backward_ckpt_workspace(esz, B, T, N, chunk_len))
+        return LPC_ERR_WORKSPACE;
+    auto run = [&](auto tag) -> int {
+        using Tt = decltype(tag);
+        BwdArgs<Tt> p{static_cast<const Tt *>(grad_y), static_cast<const Tt *>(A), static_cast<const Tt *>(zi),
+                      nullptr, static_cast<Tt *>(grad_x), static_cast<Tt *>(grad_A),
+                      static_cast<Tt *>(grad_zi), B, T, N, a_stride_b, a_stride_t};
+        return cuda_status(chunked_backward_ckpt<Tt>(p, static_cast<const Tt *>(x),
+                                                     static_cast<const Tt *>(states), chunk_len, workspace,
+                                                     workspace_bytes, s));
+    };
+    return dtype == LPC_F32 ? run(float{}) : run(double{});
+}
+
 int lpc_b200_workspace_status(const void *workspace, unsigned *status, void *stream) {
     if (!workspace || !status) return LPC_ERR_INVALID_ARGUMENT;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -158,6 +240,11 @@ int lpc_b200_workspace_status(const void *workspace, unsigned *status, void *str
                         cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return LPC_ERR_CUDA;
     return cudaStreamSynchronize(s) == cudaSuccess ? LPC_OK : LPC_ERR_CUDA;
+}
+
+int lpc_b200_set_error_word(unsigned *word) {
+    set_error_word(word);
+    return LPC_OK;
 }
 
 size_t lpc_b200_selftest_workspace_size(void) { return chunked_selftest_workspace(); }

@@ -118,6 +118,15 @@ struct ChunkParams {
     F *out;          // forward: y; backward: grad_x
     F *gA;           // backward: (B,T,N) or (B,N) when as_t == 0, or nullptr
     F *gzi;          // backward: (B,N) or nullptr
+    // Boundary-state checkpointing (forward only).  The exact entry state of
+    // every half-chunk (N values, s[i] = y[t0-1-i]) is written to ckpt at
+    // ((batch * 2G + half-chunk) * N + i) (batch: physical index, see
+    // Sig::pb; half-chunk 2g, 2g+1: the lower and upper half of chunk g).
+    // With fixonly set, the kernel instead reads those states and runs only
+    // the exact pass (phase D) of every half-chunk: y is recomputed with no
+    // map, tree or look-back work and no waits.
+    F *ckpt;
+    int fixonly;
     int64_t B, T, as_b, as_t;
     int N;
     int L;           // chunk length (multiple of the window)
@@ -133,6 +142,11 @@ struct ChunkParams {
     double *aggz;    // [nbatches][agg_z_elems]
     double *incl;    // [nbatches][N]
     unsigned spin_limit;
+    // Process-wide error word (device-visible, e.g. mapped pinned host memory)
+    // that a CTA finishing with a nonzero status word ORs that status into,
+    // so the caller learns of a bounded wait that gave up without reading the
+    // workspace; nullptr: not reported beyond the workspace.
+    unsigned *err_word;
 };
 
 // The signal a batch belongs to.
@@ -141,8 +155,9 @@ struct Sig {
     int64_t xo;      // offset of sample 0 in x, y, grad_y, grad_x (grad_A rows: xo * N)
     int64_t ao;      // offset of row 0 in A
     int64_t zo;      // offset in zi and grad_zi
-    int64_t kb, nb;  // this batch's index within the signal, batches of the signal
-    int64_t fb, fs;  // workspace index of batch m of the signal: fb + m * fs
+    int64_t kb, nb;  // this batch's index in scan order (backward: from the top), batches of the signal
+    int64_t fb, fs;  // workspace index of batch m (scan order) of the signal: fb + m * fs
+    int64_t pb;      // physical index of the signal's first batch (checkpoint states)
     int vx;          // input windows move as 16-byte vectors
 };
 
@@ -281,15 +296,17 @@ struct SmemPlan {
 };
 
 // ----------------------------------------------------------------------------
-// Window loaders.  Window w (WC steps) of chunk g (Lc steps) covers steps
-// [w*WC, w*WC+WC) of the chunk.
-// Forward: step j is time t = tb + g*Lc + w*WC + j, stored at slot j.
-// Backward: step j is time t = top-1-j (top = T - (tb + g*Lc + w*WC)),
-// stored at slot t - (top - WC) = WC-1-j.  Either way a window is a run of WC
-// consecutive coefficient rows in natural order; rows outside [0, T) read as
-// zero.  Backward windows also carry the lagged outputs
-// ys[g][r] = ypad(top-WC-NP+r), r in [0, WC+NP), natural order, with
-// ypad(-1-k) = zi[k] (zero past k = N-1).
+// Window loaders.  Both directions cut a signal on the same grid: chunk g of
+// a batch starting at sample tb covers samples [tb + g*Lc, tb + (g+1)*Lc).
+// Window w (WC steps) of chunk g holds WC consecutive coefficient rows in
+// natural order, slot j <-> row row0 + j:
+//   forward traversal (REV false): row0 = tb + g*Lc + w*WC;
+//   reverse traversal (REV true):  row0 = tb + (g+1)*Lc - (w+1)*WC, the
+//   window w*WC rows below the chunk's top (steps run from slot WC-1 down).
+// Rows at or past the end of the signal read as zero (the last chunk of a
+// signal may be partial).  Reverse windows also carry the lagged outputs
+// ys[g][r] = ypad(row0-NP+r), r in [0, WC+NP), with ypad(-1-k) = zi[k] (zero
+// past k = N-1) and zero past the end of the signal.
 // ----------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ bool is_aligned16(const void *p) {
@@ -305,16 +322,9 @@ struct Loader {
     // First row held by slot 0 of chunk g's window w, and the valid slot range.
     __device__ static void rows(const Sig &sg, int64_t tb, int Lc, int g, int w, int64_t &row0, int &lo,
                                 int &hi) {
-        if (!REV) {
-            row0 = tb + (int64_t)g * Lc + (int64_t)w * WC;
-            lo = 0;
-            hi = (int)max64(0, min64(WC, sg.T - row0));
-        } else {
-            const int64_t top = sg.T - (tb + (int64_t)g * Lc + (int64_t)w * WC);
-            row0 = top - WC;
-            lo = (int)min64(WC, max64(0, -row0));
-            hi = WC;
-        }
+        row0 = REV ? tb + (int64_t)(g + 1) * Lc - (int64_t)(w + 1) * WC : tb + (int64_t)g * Lc + (int64_t)w * WC;
+        lo = 0;
+        hi = (int)max64(0, min64(WC, sg.T - row0));
     }
 
     // Vector path: one warp per chunk (chunks warp, warp + 8, ...), so the
@@ -370,7 +380,9 @@ struct Loader {
                     const int r = (v - XV) * V;
                     T *dst = ys + (size_t)g * PY + r;
                     const int64_t j0 = row0 - NP + r;  // a multiple of V: all or none of the vector is before t = 0
-                    if (j0 >= 0) {
+                    if (j0 >= sg.T) {  // T is a multiple of V here: all of the vector is past the end
+                        *reinterpret_cast<VT *>(dst) = zero;
+                    } else if (j0 >= 0) {
                         cp_async<16>(dst, p.ysave + sg.xo + j0);
                     } else {
                         const T *zib = p.zi ? p.zi + sg.zo : nullptr;
@@ -425,7 +437,9 @@ struct Loader {
                 for (int r = lane; r < PY; r += 32) {
                     const int64_t j = row0 - NP + r;
                     T *dst = ys + (size_t)g * PY + r;
-                    if (j >= 0)  // j < top <= T
+                    if (j >= sg.T)
+                        *dst = T(0);
+                    else if (j >= 0)
                         cp_async<sizeof(T)>(dst, p.ysave + sg.xo + j);
                     else if (-1 - j < N && zib)
                         *dst = zib[-1 - j];
@@ -454,7 +468,11 @@ struct Loader {
 // Phase A: NS steps of one window segment of a chunk-map lane running KF
 // filters (ring positions U0..U0+NS-1), slots jbase.. of the window.  Bit q of
 // xmask marks filter q as the zero-state filter (the one fed the input).  One
-// broadcast load of a coefficient row feeds all KF filters of the lane.
+// broadcast load of a coefficient row feeds all KF filters of the lane.  The
+// backward runs the adjoint recurrence in transposed form over reversed time
+// (its maps come out as adjoint maps directly; the same maps built from
+// forward basis filters accumulated against grad_y lose up to two orders of
+// magnitude of accuracy in grad_x for strongly non-normal filters).
 template <typename T, int NP, int KF, bool REV, bool NEG, int WC, int U0, int NS>
 __device__ __forceinline__ void map_steps(const T *Ag, const T *xg, unsigned xmask, int jbase, T (&h)[KF][NP]) {
 #pragma unroll
@@ -564,7 +582,9 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
     T *maps = reinterpret_cast<T *>(smem + S.maps);  // [Gp][NP rows of RS | z]
     T *lbP = reinterpret_cast<T *>(smem + S.lbP);    // [2][KL][PSE]
     double *lbz = reinterpret_cast<double *>(smem + S.lbz);  // [2][KL][ZSE]
-    T *hmap = reinterpret_cast<T *>(smem + S.half);  // [G][HME]: first-half map, P[i][k] then z
+    // [G][HME]: map of the first half of each chunk in scan order (forward:
+    // the lower half, backward: the upper half), P[i][k] then z
+    T *hmap = reinterpret_cast<T *>(smem + S.half);
     double *st = reinterpret_cast<double *>(smem + S.st);    // [Gp][NP]
     double *s_in = reinterpret_cast<double *>(smem + S.sin); // [NP]
     int64_t *misc = reinterpret_cast<int64_t *>(smem + S.misc);
@@ -605,6 +625,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                     q.nb = p.bb[lo + 1] - p.bb[lo];
                     q.fb = p.bb[lo];
                     q.fs = 1;
+                    q.pb = p.bb[lo];
                 } else {
                     // uniform: batch kb of every signal before batch kb+1 of any
                     const int64_t b = t % p.B;
@@ -616,10 +637,11 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                     q.nb = p.nbps;
                     q.fb = b;
                     q.fs = p.B;
+                    q.pb = b * p.nbps;
                 }
                 // vector input windows need an aligned signal start and a
-                // length of whole vectors: backward windows start at T - pos,
-                // and a window's last vector must not reach past the signal
+                // length of whole vectors (a window's last vector must not
+                // reach past the signal)
                 q.vx = (WD * (int)sizeof(T)) % 16 == 0 && (q.T * (int64_t)sizeof(T)) % 16 == 0 &&
                        is_aligned16<T>(p.in + q.xo) && (!p.ysave || is_aligned16<T>(p.ysave + q.xo));
                 *sgs = q;
@@ -627,19 +649,33 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
         }
         __syncthreads();
         const int64_t ticket = misc[0];
-        if (ticket >= nbatches) break;
+        if (ticket >= nbatches) {
+            if (tid == 0 && p.err_word) {
+                // this CTA's own give-ups are in the status word by now
+                const unsigned st_now = ld_acquire(p.status);
+                if (st_now) {
+                    volatile unsigned *ew = p.err_word;
+                    *ew = *ew | st_now;
+                }
+            }
+            break;
+        }
         const Sig sg = *sgs;
-        const int64_t kb = sg.kb;  // batch index within the signal
-        const int64_t tb = kb * (int64_t)G * L;  // first step of the batch
+        // scan order: the forward walks a signal's batches from its start, the
+        // backward from its end; both cut the signal on the same grid
+        const int64_t kb = sg.kb;                      // batch index in scan order
+        const int64_t jb = REV ? sg.nb - 1 - kb : kb;  // batch index from the signal's start
+        const int64_t tb = jb * (int64_t)G * L;        // first sample of the batch
         const int64_t rem = sg.T - tb;
         const int Gb = (int)min64(G, (rem + L - 1) / L);
 
         // ------------------------------------------------------------ phase A
-        // chunk maps: N basis filters + one zero-state filter per chunk
+        // chunk maps: N basis filters + one zero-state filter per chunk, in
+        // scan order (backward: the adjoint recurrence over reversed time)
         if (p.loader == kLoadElem && N < NP)  // padded coefficient columns must read as zero
             for (int e = tid; e < 2 * G * GSA; e += THREADS)
                 if ((e % GSA) % NP >= N) Abuf[e] = T(0);
-        const bool active = grp < Gb;
+        const bool active = grp < Gb && !p.fixonly;
         unsigned xmask = 0;
         T h[KF][NP];
 #pragma unroll
@@ -649,44 +685,49 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
 #pragma unroll
             for (int j = 0; j < NP; ++j) h[q][j] = (active && f < N && j == state_slot<REV, NP>(f)) ? T(1) : T(0);
         }
-
-        LA::load(p, sg, tb, Gb, L, 0, Abuf, ibuf, nullptr, false);
-        cp_async_commit();
-        for (int w = 0; w < nwin; ++w) {
-            const int s = w & 1;
-            if (w + 1 < nwin)
-                LA::load(p, sg, tb, Gb, L, w + 1, Abuf + (size_t)(s ^ 1) * G * GSA, ibuf + (size_t)(s ^ 1) * G * W,
-                         nullptr, false);
+        if (!p.fixonly) {
+            LA::load(p, sg, tb, Gb, L, 0, Abuf, ibuf, nullptr, false);
             cp_async_commit();
-            cp_async_wait<1>();
-            __syncthreads();
-            if (active) {
-                if (w == nwin / 2) {
-                    // the state after the first half of the chunk: the lane's
-                    // columns of the half map (or its z)
+            for (int w = 0; w < nwin; ++w) {
+                const int s = w & 1;
+                if (w + 1 < nwin)
+                    LA::load(p, sg, tb, Gb, L, w + 1, Abuf + (size_t)(s ^ 1) * G * GSA,
+                             ibuf + (size_t)(s ^ 1) * G * W, nullptr, false);
+                cp_async_commit();
+                cp_async_wait<1>();
+                __syncthreads();
+                if (active) {
+                    if (w == nwin / 2) {
+                        // the state after the first half of the chunk (in scan
+                        // order): the lane's columns of the half map (or its z)
 #pragma unroll
-                    for (int q = 0; q < KF; ++q)
-                        put_map_column<T, NP, REV>(hmap + (size_t)grp * HME, NP, h[q], kk * KF + q, N);
-                }
-                const T *Ag = Abuf + (size_t)s * G * GSA + (size_t)grp * GSA;
-                const T *xg = ibuf + (size_t)s * G * W + (size_t)grp * W;
+                        for (int q = 0; q < KF; ++q)
+                            put_map_column<T, NP, REV>(hmap + (size_t)grp * HME, NP, h[q], kk * KF + q, N);
+                    }
+                    const T *Ag = Abuf + (size_t)s * G * GSA + (size_t)grp * GSA;
+                    const T *xg = ibuf + (size_t)s * G * W + (size_t)grp * W;
 #pragma unroll 1
-                for (int blk = 0; blk < W / NP; ++blk)
-                    map_steps<T, NP, KF, REV, NEG, W, 0, NP>(Ag, xg, xmask, blk * NP, h);
+                    for (int blk = 0; blk < W / NP; ++blk)
+                        map_steps<T, NP, KF, REV, NEG, W, 0, NP>(Ag, xg, xmask, blk * NP, h);
+                }
+                __syncthreads();
             }
+            cp_async_wait<0>();
             __syncthreads();
         }
-        cp_async_wait<0>();
-        __syncthreads();
 
         // ------------------------------------------------------------ phase B
-        // maps (aliasing the window buffers): zero, then column k of chunk g's
-        // P from lane k, z from the zero-state lane; identity beyond Gb.
+        // tree leaves (aliasing the window buffers): zero, then the chunk maps
+        // (column k of a chunk's P from lane k, z from the zero-state lane),
+        // identity beyond Gb.  Leaf 0 is the chunk scanned first: forward,
+        // chunk g is leaf g; backward (from the top), chunk g is leaf Gb-1-g.
+        if (!p.fixonly) {
         for (int e = tid; e < Gp * MS; e += THREADS) maps[e] = T(0);
         __syncthreads();
         if (active) {
 #pragma unroll
-            for (int q = 0; q < KF; ++q) put_map_column<T, NP, REV>(maps + (size_t)grp * MS, RS, h[q], kk * KF + q, N);
+            for (int q = 0; q < KF; ++q)
+                put_map_column<T, NP, REV>(maps + (size_t)(REV ? Gb - 1 - grp : grp) * MS, RS, h[q], kk * KF + q, N);
         }
         for (int e = tid; e < (Gp - Gb) * N; e += THREADS) {
             const int g = Gb + e / N;
@@ -899,11 +940,18 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                 __syncthreads();
             }
         }
+        }  // !fixonly
 
         // ------------------------------------------------------------ phase D
-        // fix-up: one lane per half-chunk re-runs it from its exact entry
-        // state (second halves: the first half's map applied to the chunk's
-        // entry state, in FP64)
+        // fix-up: one lane per half-chunk (lane 2g: the lower half of chunk g,
+        // lane 2g+1: the upper half) re-runs it from its exact entry state, in
+        // scan order.  Forward: the lower half starts from the chunk's entry
+        // state, the upper half from the first half's map applied to it.
+        // Backward: the upper half starts from the adjoint state at the
+        // chunk's top, the lower half from the upper half's adjoint map
+        // applied to it.  The maps are applied in FP64.  A checkpointed
+        // forward records every half-chunk's entry state; a fix-only launch
+        // starts each half-chunk from the recorded one.
         const int Gd = 2 * Gb;  // half-chunks of the batch
         if (p.loader == kLoadElem && N < NP)
             for (int e = tid; e < 2 * 2 * G * GSD; e += THREADS)
@@ -911,19 +959,31 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
         const bool fix = tid < Gd;
         {
             const int g = tid >> 1;
-            const double *sg = st + (size_t)g * NP;
-            if (fix && (tid & 1)) {
+            const int slot = !fix ? 0 : (REV ? Gb - 1 - g : g);
+            const double *sv = st + (size_t)slot * NP;
+            const bool via_half = REV ? (tid & 1) == 0 : (tid & 1) == 1;
+            T *ck = (!REV && p.ckpt && fix) ? p.ckpt + ((size_t)(sgs->pb + jb) * 2 * G + tid) * N : nullptr;
+            if (!REV && p.fixonly) {
+#pragma unroll
+                for (int i = 0; i < NP; ++i) h[0][state_slot<REV, NP>(i)] = (ck && i < N) ? ck[i] : T(0);
+            } else if (fix && via_half) {
                 const T *Hg = hmap + (size_t)g * HME;
 #pragma unroll
                 for (int i = 0; i < NP; ++i) {
                     double v = (double)Hg[NP * NP + i];
 #pragma unroll
-                    for (int k = 0; k < NP; ++k) v = fma((double)Hg[i * NP + k], sg[k], v);
+                    for (int k = 0; k < NP; ++k) v = fma((double)Hg[i * NP + k], sv[k], v);
                     h[0][state_slot<REV, NP>(i)] = i < N ? (T)v : T(0);
                 }
             } else {
 #pragma unroll
-                for (int i = 0; i < NP; ++i) h[0][state_slot<REV, NP>(i)] = (fix && i < N) ? (T)sg[i] : T(0);
+                for (int i = 0; i < NP; ++i) h[0][state_slot<REV, NP>(i)] = (fix && i < N) ? (T)sv[i] : T(0);
+            }
+            if (ck && !p.fixonly) {
+                // boundary-state checkpoint: the half-chunk's exact entry state
+#pragma unroll
+                for (int i = 0; i < NP; ++i)
+                    if (i < N) ck[i] = h[0][state_slot<REV, NP>(i)];
             }
         }
         const bool ti = REV && p.gA && p.as_t == 0;
@@ -960,25 +1020,22 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                 }
             }
             __syncthreads();
-            // flush the window's outputs (obuf is indexed by step)
+            // flush the window's outputs (obuf is indexed by step): step j of
+            // half-chunk g is sample tb + g*LH + w*WD + j forward and
+            // tb + (g+1)*LH - w*WD - 1 - j backward
             for (int e = tid; e < Gd * WD; e += THREADS) {
                 const int g = e / WD;
                 const int j = e - g * WD;
-                const int64_t pos = tb + (int64_t)g * LH + (int64_t)w * WD + j;  // step index
-                if (pos < sg.T) {
-                    const int64_t t = REV ? sg.T - 1 - pos : pos;
-                    p.out[sg.xo + t] = obuf[e];
-                } else if (REV && p.gzi && pos - sg.T < N) {
-                    // steps past t = 0 carry the adjoint into the initial conditions
-                    p.gzi[sg.zo + (pos - sg.T)] = obuf[e];
-                }
+                const int64_t t = REV ? tb + (int64_t)(g + 1) * LH - (int64_t)w * WD - 1 - j
+                                      : tb + (int64_t)g * LH + (int64_t)w * WD + j;
+                if (t < sg.T) p.out[sg.xo + t] = obuf[e];
             }
             if (REV && p.gA && !ti) {
                 // one warp per half-chunk: row t = top-WD+rr has grad_x[t] =
                 // obuf[g][WD-1-rr] and y[t-1-i] = ys[g][rr+NP-1-i]
                 const T sgn = NEG ? T(1) : T(-1);
                 for (int g = tid >> 5; g < Gd; g += THREADS / 32) {
-                    const int64_t top = sg.T - (tb + (int64_t)g * LH + (int64_t)w * WD);
+                    const int64_t top = tb + (int64_t)(g + 1) * LH - (int64_t)w * WD;
                     const T *og = obuf + g * WD + (WD - 1);
                     const T *yg = ys + g * PYD + NP - 1;
                     if (gA_vec) {
@@ -987,12 +1044,12 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                         constexpr int QR = NP / V > 0 ? NP / V : 1;  // vectors per row (gA_vec: NP % V == 0)
                         constexpr int QPC = WD * QR;                 // vectors per half-chunk window
                         using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-                        const int64_t r0 = sg.xo + top - WD;  // row of slot 0; rows with t < 0 are skipped
+                        const int64_t r0 = sg.xo + top - WD;  // row of slot 0; rows past the signal are skipped
 #pragma unroll
                         for (int k = 0; k < (QPC + 31) / 32; ++k) {
                             const int v = lane + 32 * k;
                             const int rr = v / QR;
-                            if ((QPC % 32 != 0 && v >= QPC) || top - WD + rr < 0) continue;
+                            if ((QPC % 32 != 0 && v >= QPC) || top - WD + rr >= sg.T) continue;
                             const int i0 = (v - rr * QR) * V;
                             const T gx = sgn * og[-rr];
                             const T *yq = yg + rr - i0;
@@ -1007,7 +1064,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
                             const int rr = e / N;
                             const int i = e - rr * N;
                             const int64_t t = top - WD + rr;
-                            if (t < 0) continue;
+                            if (t >= sg.T) continue;
                             p.gA[(sg.xo + t) * N + i] = sgn * og[-rr] * yg[rr - i];
                         }
                     }
@@ -1016,15 +1073,12 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
             __syncthreads();
         }
         cp_async_wait<0>();
-        // grad_zi entries beyond the padded steps of the signal's last chunk are
-        // still pending in the exit state of its second half
-        if (REV && p.gzi && kb + 1 == sg.nb && tid == Gd - 1) {
-            const int64_t npad = tb + (int64_t)Gb * L - sg.T;  // steps of the chunk with t < 0
+        // the lower half of the signal's first chunk ends at t = 0 holding the
+        // adjoint of the initial conditions (pending gradients of y[-1-i])
+        if (REV && p.gzi && jb == 0 && tid == 0) {
 #pragma unroll
-            for (int i = 0; i < NP; ++i) {
-                const int64_t k = npad + i;
-                if (i < N && k < N) p.gzi[sg.zo + k] = h[0][state_slot<REV, NP>(i)];
-            }
+            for (int i = 0; i < NP; ++i)
+                if (i < N) p.gzi[sg.zo + i] = h[0][state_slot<REV, NP>(i)];
         }
     }
 }
@@ -1040,6 +1094,9 @@ inline int64_t default_chunk(int64_t T) { return T < 65536 ? kChunkLen / 2 : (T 
 
 // Process-wide target chunk length (the autotuner's knob; 0 = default).
 std::atomic<int64_t> g_chunk_target{0};
+
+// Process-wide error word of the chunked kernels (see ChunkParams::err_word).
+std::atomic<unsigned *> g_err_word{nullptr};
 constexpr int kMaxChunksPerBatch = 64;
 
 inline int threads_for(int) { return 256; }  // scan group: one group of phase-A lanes per chunk
@@ -1053,11 +1110,13 @@ struct Plan {
 // Chunks per batch: one group of N+1 lanes per chunk, capped so that the
 // shared memory of a CTA fits the occupancy the kernel is built for
 // (ctas_per_sm: two CTAs per SM up to order 16 and for fp64, three above).
-inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N, int64_t dflt = 0) {
+// `force` > 0 fixes the chunk length (a checkpointed forward and its
+// backward must cut the signal identically).
+inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N, int64_t dflt = 0, int64_t force = 0) {
     Plan pl;
     pl.NP = padded_order(N);
     const int W = window_for(pl.NP);
-    const int64_t want = g_chunk_target.load(std::memory_order_relaxed);
+    const int64_t want = force > 0 ? force : g_chunk_target.load(std::memory_order_relaxed);
     // default by signal length: short signals want more batches in flight,
     // long ones fewer look-back hops per sample
     const int64_t target = want > 0 ? want : (dflt > 0 ? dflt : default_chunk(T));
@@ -1146,12 +1205,15 @@ ChunkParams<T> base_params(const Plan &pl, int64_t B, int64_t T_, int64_t N, voi
     p.aggz = reinterpret_cast<double *>(w + l.aggz);
     p.incl = reinterpret_cast<double *>(w + l.incl);
     p.spin_limit = 1u << 20;  // each poll is an L2 round trip: about a second in total
+    p.err_word = g_err_word.load(std::memory_order_acquire);
     return p;
 }
 
 }  // namespace
 
 bool chunked_supported(int64_t N) { return N >= 1 && N <= 32; }
+
+void set_error_word(unsigned *word) { g_err_word.store(word, std::memory_order_release); }
 
 void set_chunk_target(int64_t samples) {
     g_chunk_target.store(samples <= 0 ? 0 : (samples < 32 ? 32 : (samples > 4096 ? 4096 : samples)),
@@ -1213,6 +1275,118 @@ cudaError_t chunked_backward(const BwdArgs<T> &a, bool neg, void *ws, size_t ws_
     if (e != cudaSuccess || !a.gA || a.a_stride_t != 0) return e;
     return ti_grad_a<T>(a.gx, a.y, a.zi, a.gA, a.B, a.T, a.N, neg, st);  // reads the grad_x just written
 }
+
+// ----------------------------------------------------------------------------
+// Boundary-state checkpointing: the forward keeps the exact entry state of
+// every half-chunk (N values per half-chunk, batch-major in the plan's layout)
+// beside y, so that y need not be kept for the backward.  The backward first
+// recomputes y from those states and x with a fix-only launch of the forward
+// kernel (the exact pass alone: every half-chunk independent, no maps, no
+// look-back), into its workspace, then runs the fused backward on it.  Both
+// calls take the same chunk length, which fixes the plan (the chunk-length
+// setting may change in between).
+// ----------------------------------------------------------------------------
+namespace {
+
+struct CkptLayout {
+    Plan pl;
+    WsLayout l;
+    size_t ybuf, total;
+};
+
+inline CkptLayout ckpt_layout(size_t esz, int64_t B, int64_t T, int64_t N, int64_t chunk) {
+    CkptLayout c;
+    c.pl = make_plan(esz, B, T, N, 0, chunk);
+    c.l = ws_layout(esz, c.pl.nbatches, N);
+    c.ybuf = c.l.total;
+    c.total = align256(c.ybuf + (size_t)B * T * esz);
+    return c;
+}
+
+}  // namespace
+
+int64_t chunked_checkpoint_chunk(size_t esz, int64_t T, int64_t N) { return make_plan(esz, 1, T, N).L; }
+
+int64_t chunked_checkpoint_elems(size_t esz, int64_t B, int64_t T, int64_t N, int64_t chunk) {
+    if (!chunked_supported(N) || chunk <= 0) return 0;
+    const Plan pl = make_plan(esz, B, T, N, 0, chunk);
+    return pl.nbatches * 2 * pl.G * N;
+}
+
+size_t chunked_forward_ckpt_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t chunk) {
+    if (!chunked_supported(N) || chunk <= 0) return 0;
+    return ws_layout(esz, make_plan(esz, B, T, N, 0, chunk).nbatches, N).total;
+}
+
+size_t chunked_backward_ckpt_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t chunk) {
+    if (!chunked_supported(N) || chunk <= 0) return 0;
+    return ckpt_layout(esz, B, T, N, chunk).total;
+}
+
+template <typename T>
+cudaError_t chunked_forward_ckpt(const FwdArgs<T> &a, T *states, int64_t chunk, void *ws, size_t ws_bytes,
+                                 cudaStream_t st) {
+    const Plan pl = make_plan(sizeof(T), a.B, a.T, a.N, 0, chunk);
+    const WsLayout l = ws_layout(sizeof(T), pl.nbatches, a.N);
+    if (ws_bytes < l.total) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(ws, 0, l.aggP, st);  // header + flags
+    if (e != cudaSuccess) return e;
+    ChunkParams<T> p = base_params<T>(pl, a.B, a.T, a.N, ws);
+    p.in = a.x;
+    p.A = a.A;
+    p.as_b = a.a_stride_b;
+    p.as_t = a.a_stride_t;
+    p.zi = a.zi;
+    p.out = a.y;
+    p.ckpt = states;
+    return dispatch<T, false, false>(p, pl.NP, st);
+}
+
+template <typename T>
+cudaError_t chunked_backward_ckpt(const BwdArgs<T> &a, const T *x, const T *states, int64_t chunk, void *ws,
+                                  size_t ws_bytes, cudaStream_t st) {
+    const CkptLayout c = ckpt_layout(sizeof(T), a.B, a.T, a.N, chunk);
+    if (ws_bytes < c.total) return cudaErrorInvalidValue;
+    T *y = reinterpret_cast<T *>(static_cast<unsigned char *>(ws) + c.ybuf);
+    // 1. y from the recorded half-chunk states (only the ticket counter and
+    //    the status word of the workspace are used)
+    cudaError_t e = cudaMemsetAsync(ws, 0, c.l.aggP, st);
+    if (e != cudaSuccess) return e;
+    ChunkParams<T> p = base_params<T>(c.pl, a.B, a.T, a.N, ws);
+    p.in = x;
+    p.A = a.A;
+    p.as_b = a.a_stride_b;
+    p.as_t = a.a_stride_t;
+    p.zi = a.zi;
+    p.out = y;
+    p.ckpt = const_cast<T *>(states);
+    p.fixonly = 1;
+    e = dispatch<T, false, false>(p, c.pl.NP, st);
+    if (e != cudaSuccess) return e;
+    // 2. the fused backward on it, with the same plan
+    e = cudaMemsetAsync(ws, 0, c.l.aggP, st);
+    if (e != cudaSuccess) return e;
+    ChunkParams<T> q = base_params<T>(c.pl, a.B, a.T, a.N, ws);
+    q.in = a.gy;
+    q.A = a.A;
+    q.as_b = a.a_stride_b;
+    q.as_t = a.a_stride_t;
+    q.zi = a.zi;
+    q.ysave = y;
+    q.out = a.gx;
+    q.gA = a.gA;
+    q.gzi = a.gzi;
+    return dispatch<T, true, false>(q, c.pl.NP, st);
+}
+
+template cudaError_t chunked_forward_ckpt<float>(const FwdArgs<float> &, float *, int64_t, void *, size_t,
+                                                 cudaStream_t);
+template cudaError_t chunked_forward_ckpt<double>(const FwdArgs<double> &, double *, int64_t, void *, size_t,
+                                                  cudaStream_t);
+template cudaError_t chunked_backward_ckpt<float>(const BwdArgs<float> &, const float *, const float *, int64_t,
+                                                  void *, size_t, cudaStream_t);
+template cudaError_t chunked_backward_ckpt<double>(const BwdArgs<double> &, const double *, const double *,
+                                                   int64_t, void *, size_t, cudaStream_t);
 
 // ----------------------------------------------------------------------------
 // Ragged batches: nsig signals concatenated along time, signal s occupying

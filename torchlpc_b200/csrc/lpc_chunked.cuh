@@ -10,6 +10,8 @@ namespace lpcb {
 constexpr int64_t kMaxOrder = 1024;
 
 bool chunked_supported(int64_t N);
+// Process-wide error word the chunked kernels OR a nonzero status into.
+void set_error_word(unsigned *word);
 // Target chunk length of the chunked scan (process-wide; <= 0 restores the
 // default, chosen by signal length; chunk_target() then returns 0); the plan
 // rounds it to an even number of windows.
@@ -28,6 +30,19 @@ template <typename T>
 cudaError_t chunked_backward_ragged(const T *gy, const T *A, const int64_t *off, const T *zi, const T *y, T *gx,
                                     T *gA, T *gzi, int64_t nsig, int64_t S, int64_t N, void *ws, size_t ws_bytes,
                                     cudaStream_t st);
+
+// Boundary-state checkpointing (time-varying coefficients): the forward keeps
+// every chunk's entry state, the backward recomputes y from them and x.
+int64_t chunked_checkpoint_chunk(size_t esz, int64_t T, int64_t N);
+int64_t chunked_checkpoint_elems(size_t esz, int64_t B, int64_t T, int64_t N, int64_t chunk);
+size_t chunked_forward_ckpt_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t chunk);
+size_t chunked_backward_ckpt_workspace(size_t esz, int64_t B, int64_t T, int64_t N, int64_t chunk);
+template <typename T>
+cudaError_t chunked_forward_ckpt(const FwdArgs<T> &a, T *states, int64_t chunk, void *ws, size_t ws_bytes,
+                                 cudaStream_t st);
+template <typename T>
+cudaError_t chunked_backward_ckpt(const BwdArgs<T> &a, const T *x, const T *states, int64_t chunk, void *ws,
+                                  size_t ws_bytes, cudaStream_t st);
 
 // Failure detection: a launch whose look-back wait runs out (no GPU fault).
 size_t chunked_selftest_workspace();

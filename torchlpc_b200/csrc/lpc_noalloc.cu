@@ -13,9 +13,11 @@
 // The array is a file-scope __device__ variable, so every GPU that loads this
 // library holds kStaticScratchBytes of device memory until the process exits.
 // Its host-side name is only a stand-in for the symbol: the device address is
-// looked up with cudaGetSymbolAddress once per device, on the first call made
-// while that device is current, and cached.
-#include <mutex>
+// looked up with cudaGetSymbolAddress on every call, for the device (and
+// context) current at that moment.  The lookup allocates nothing; the first
+// one on a device also loads the module there, which is why that first call
+// must come before any stream capture.  Nothing is cached, so a device reset
+// or another context made current between calls cannot leave a stale address.
 
 #include "lpc_chunked.cuh"
 
@@ -27,25 +29,14 @@ namespace {
 // million samples per call at order 16 (longer signals use longer chunks; the
 // scratch grows with the number of batches and with N^2).
 constexpr size_t kStaticScratchBytes = size_t(8) << 20;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
-std::mutex g_setup_mutex;
-void *g_scratch_addr[kMaxDevices] = {nullptr};
-
-// Device address of the scratch array on the current device (looked up once).
+// Device address of the scratch array in the current context.
 int scratch_for_current_device(void **out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return LPC_ERR_CUDA;
-    if (dev < 0 || dev >= kMaxDevices) return LPC_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (g_scratch_addr[dev] == nullptr) {
-        void *ptr = nullptr;
-        if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || ptr == nullptr) return LPC_ERR_CUDA;
-        g_scratch_addr[dev] = ptr;
-    }
-    *out = g_scratch_addr[dev];
+    void *ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || ptr == nullptr) return LPC_ERR_CUDA;
+    *out = ptr;
     return LPC_OK;
 }
 
@@ -55,9 +46,13 @@ int run(const void *x, const void *A, const void *zi, void *y, int64_t B, int64_
     FwdArgs<T> p{static_cast<const T *>(x), static_cast<const T *>(A), static_cast<const T *>(zi),
                  static_cast<T *>(y), B, T_, N, sb, st};
     // chunked_forward clears the counter, status word and flags of the scratch
-    // on `stream` before the kernel runs; the rest is written before it is read
-    return chunked_forward<T>(p, false, scratch, kStaticScratchBytes, stream) == cudaSuccess ? LPC_OK
-                                                                                              : LPC_ERR_CUDA;
+    // on `stream` before the kernel runs; the rest is written before it is read.
+    // It refuses a plan larger than the scratch with cudaErrorInvalidValue (the
+    // chunk-length setting changed since the size check): report that as the
+    // size error it is.
+    const cudaError_t e = chunked_forward<T>(p, false, scratch, kStaticScratchBytes, stream);
+    if (e == cudaErrorInvalidValue) return LPC_ERR_WORKSPACE;
+    return e == cudaSuccess ? LPC_OK : LPC_ERR_CUDA;
 }
 
 }  // namespace
@@ -79,4 +74,13 @@ extern "C" int lpc_b200_forward_noalloc(int dtype, const void *x, const void *A,
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (dtype == LPC_F32) return run<float>(x, A, zi, y, B, T, N, a_stride_b, a_stride_t, scratch, s);
     return run<double>(x, A, zi, y, B, T, N, a_stride_b, a_stride_t, scratch, s);
+}
+
+extern "C" int lpc_b200_noalloc_status(unsigned *status, void *stream) {
+    if (!status) return LPC_ERR_INVALID_ARGUMENT;
+    void *scratch = nullptr;
+    const int rc = scratch_for_current_device(&scratch);
+    if (rc != LPC_OK) return rc;
+    // the status word follows the ticket counter at the start of the scratch
+    return lpc_b200_workspace_status(scratch, status, stream);
 }

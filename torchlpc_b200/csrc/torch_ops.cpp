@@ -7,6 +7,8 @@
 // only: there is no CPU implementation and no fallback.
 #include <Python.h>
 #include <ATen/ATen.h>
+#include <mutex>
+#include <sstream>
 #include <c10/cuda/CUDAGuard.h>
 #include <c10/cuda/CUDAStream.h>
 #include <torch/library.h>
@@ -23,6 +25,43 @@ PyObject *PyInit__C(void) {
 }
 
 namespace {
+
+// Error word: one pinned host word (directly addressable by every device
+// under unified addressing), installed as the library's process-wide error
+// word on the first operator call.  A chunked kernel whose bounded wait gave
+// up ORs its status into it; every operator reads it on entry (a plain host
+// read, no synchronisation) and raises for the earlier call whose outputs are
+// invalid.  check_status() synchronises first.
+volatile unsigned *g_err_host = nullptr;
+std::once_flag g_err_once;
+
+void ensure_error_word() {
+    std::call_once(g_err_once, [] {
+        // leaked on purpose: the kernels may write it until the process exits
+        auto *t = new at::Tensor(at::zeros({1}, at::TensorOptions().dtype(at::kInt).pinned_memory(true)));
+        g_err_host = reinterpret_cast<volatile unsigned *>(t->data_ptr());
+        lpc_b200_set_error_word(const_cast<unsigned *>(g_err_host));
+    });
+}
+
+unsigned take_error_word() {
+    ensure_error_word();
+    const unsigned w = *g_err_host;
+    if (w) *g_err_host = 0;
+    return w;
+}
+
+void raise_pending() {
+    const unsigned w = take_error_word();
+    if (w) {
+        std::ostringstream m;
+        m << "torchlpc_b200: a bounded device-side wait of a chunked kernel gave up in an earlier call "
+             "(status word 0x"
+          << std::hex << w << "; 1: a predecessor's flag never appeared, 2: inconsistent flags, 8: a ragged "
+          << "signal with a negative length); the outputs of that call are invalid";
+        TORCH_CHECK(false, m.str());
+    }
+}
 
 int dtype_code(const at::Tensor &t) {
     if (t.scalar_type() == at::kFloat) return LPC_F32;
@@ -76,6 +115,7 @@ Coeffs coeffs(const at::Tensor &A, int64_t B, int64_t T, int64_t N, bool allow_t
 
 at::Tensor lpc(const at::Tensor &x, const at::Tensor &A, const c10::optional<at::Tensor> &zi_opt,
                int64_t algo) {
+    raise_pending();
     TORCH_CHECK(x.is_floating_point() || x.is_complex(), "Input must be floating point or complex");
     TORCH_CHECK(A.scalar_type() == x.scalar_type(),
                 "Coefficients must have the same scalar type as input");
@@ -115,6 +155,7 @@ at::Tensor lpc(const at::Tensor &x, const at::Tensor &A, const c10::optional<at:
 std::tuple<at::Tensor, at::Tensor, at::Tensor> lpc_backward(
     const at::Tensor &grad_y, const at::Tensor &A, const c10::optional<at::Tensor> &zi_opt,
     const at::Tensor &y, bool need_A, bool need_zi, int64_t algo) {
+    raise_pending();
     TORCH_CHECK(grad_y.dim() == 2 && y.dim() == 2 && grad_y.sizes() == y.sizes(),
                 "grad_y and y must be (B, T)");
     TORCH_CHECK(A.scalar_type() == y.scalar_type() && grad_y.scalar_type() == y.scalar_type(),
@@ -150,6 +191,7 @@ std::tuple<at::Tensor, at::Tensor, at::Tensor> lpc_backward(
 
 at::Tensor scan(const at::Tensor &input, const at::Tensor &weights, const c10::optional<at::Tensor> &init_opt,
                 int64_t algo) {
+    raise_pending();
     TORCH_CHECK(input.is_floating_point() || input.is_complex(),
                 "Input must be floating point or complex");
     TORCH_CHECK(weights.scalar_type() == input.scalar_type(),
@@ -185,6 +227,7 @@ at::Tensor scan(const at::Tensor &input, const at::Tensor &weights, const c10::o
 std::tuple<at::Tensor, at::Tensor, at::Tensor> scan_backward(
     const at::Tensor &grad_out, const at::Tensor &decay, const c10::optional<at::Tensor> &init_opt,
     const at::Tensor &out, bool need_decay, bool need_init, int64_t algo) {
+    raise_pending();
     TORCH_CHECK(grad_out.dim() == 2 && grad_out.sizes() == out.sizes() && decay.sizes() == out.sizes(),
                 "grad_out, decay and out must be (B, T)");
     check_cuda(grad_out, "grad_out");
@@ -224,6 +267,7 @@ void check_ragged(const at::Tensor &x, const at::Tensor &A, const at::Tensor &of
 
 at::Tensor lpc_ragged(const at::Tensor &x, const at::Tensor &A, const at::Tensor &offsets,
                       const c10::optional<at::Tensor> &zi_opt) {
+    raise_pending();
     check_ragged(x, A, offsets);
     const int64_t S = x.size(0), N = A.size(1), nsig = offsets.size(0) - 1;
     at::Tensor zi;
@@ -249,6 +293,7 @@ at::Tensor lpc_ragged(const at::Tensor &x, const at::Tensor &A, const at::Tensor
 std::tuple<at::Tensor, at::Tensor, at::Tensor> lpc_backward_ragged(
     const at::Tensor &grad_y, const at::Tensor &A, const at::Tensor &offsets,
     const c10::optional<at::Tensor> &zi_opt, const at::Tensor &y, bool need_A, bool need_zi) {
+    raise_pending();
     check_ragged(y, A, offsets);
     TORCH_CHECK(grad_y.sizes() == y.sizes() && grad_y.scalar_type() == y.scalar_type(),
                 "grad_y and y must both be (S,) of one dtype");
@@ -277,6 +322,102 @@ std::tuple<at::Tensor, at::Tensor, at::Tensor> lpc_backward_ragged(
     return {gx, gA, gzi};
 }
 
+// Boundary-state checkpointing: the forward returns y and the chunk entry
+// states; the backward takes x and those states instead of y.
+std::tuple<at::Tensor, at::Tensor> lpc_checkpointed(const at::Tensor &x, const at::Tensor &A,
+                                                    const c10::optional<at::Tensor> &zi_opt, int64_t chunk) {
+    raise_pending();
+    TORCH_CHECK(x.is_floating_point(), "Input must be floating point");
+    TORCH_CHECK(A.scalar_type() == x.scalar_type(), "Coefficients must have the same scalar type as input");
+    TORCH_CHECK(x.dim() == 2 && A.dim() == 3, "checkpointed filter: x (B,T), A (B,T,order)");
+    check_cuda(x, "x");
+    check_cuda(A, "A");
+    const int64_t B = x.size(0), T = x.size(1), N = A.size(-1);
+    at::Tensor zi;
+    if (zi_opt.has_value() && zi_opt->defined()) {
+        zi = zi_opt->contiguous();
+        TORCH_CHECK(zi.scalar_type() == x.scalar_type() && zi.dim() == 2 && zi.size(0) == B && zi.size(1) == N,
+                    "Initial conditions must be (B, order) of the input's dtype");
+    }
+    const int dt = dtype_code(x);
+    const c10::cuda::CUDAGuard guard(x.device());
+    Coeffs c = coeffs(A, B, T, N, false);
+    at::Tensor xc = x.contiguous();
+    at::Tensor y = at::empty({B, T}, x.options());
+    const int64_t ne = lpc_b200_checkpoint_elems(dt, B, T, N, chunk);
+    TORCH_CHECK(ne > 0 || B * T == 0, "torchlpc_b200::lpc_checkpointed: unsupported order or chunk length");
+    at::Tensor states = at::empty({std::max<int64_t>(ne, 0)}, x.options());
+    const size_t wsb = lpc_b200_forward_checkpointed_workspace_size(dt, B, T, N, chunk);
+    at::Tensor ws = workspace(wsb, x);
+    check_status(lpc_b200_forward_checkpointed(dt, xc.data_ptr(), c.t.data_ptr(), ptr_or_null(zi), y.data_ptr(),
+                                               states.data_ptr(), B, T, N, c.sb, c.st, chunk, ptr_or_null(ws),
+                                               wsb, c10::cuda::getCurrentCUDAStream().stream()),
+                 "lpc_checkpointed");
+    return {y, states};
+}
+
+std::tuple<at::Tensor, at::Tensor, at::Tensor> lpc_backward_checkpointed(
+    const at::Tensor &grad_y, const at::Tensor &A, const c10::optional<at::Tensor> &zi_opt, const at::Tensor &x,
+    const at::Tensor &states, int64_t chunk, bool need_A, bool need_zi) {
+    raise_pending();
+    TORCH_CHECK(grad_y.dim() == 2 && x.dim() == 2 && grad_y.sizes() == x.sizes(), "grad_y and x must be (B, T)");
+    TORCH_CHECK(A.scalar_type() == x.scalar_type() && grad_y.scalar_type() == x.scalar_type() &&
+                    states.scalar_type() == x.scalar_type(),
+                "dtype mismatch");
+    check_cuda(grad_y, "grad_y");
+    check_cuda(A, "A");
+    check_cuda(x, "x");
+    check_cuda(states, "states");
+    const int64_t B = x.size(0), T = x.size(1), N = A.size(-1);
+    at::Tensor zi;
+    if (zi_opt.has_value() && zi_opt->defined()) {
+        zi = zi_opt->contiguous();
+        TORCH_CHECK(zi.dim() == 2 && zi.size(0) == B && zi.size(1) == N, "zi must be (B, order)");
+    }
+    const int dt = dtype_code(x);
+    TORCH_CHECK(states.numel() == std::max<int64_t>(lpc_b200_checkpoint_elems(dt, B, T, N, chunk), 0),
+                "checkpoint states do not match (B, T, order, chunk length)");
+    const c10::cuda::CUDAGuard guard(x.device());
+    Coeffs c = coeffs(A, B, T, N, false);
+    at::Tensor gyc = grad_y.contiguous(), xc = x.contiguous(), sc = states.contiguous();
+    at::Tensor gx = at::empty({B, T}, x.options());
+    at::Tensor gA = need_A ? at::empty({B, T, N}, x.options()) : at::Tensor();
+    at::Tensor gzi = need_zi ? at::empty({B, N}, x.options()) : at::Tensor();
+    const size_t wsb = lpc_b200_backward_checkpointed_workspace_size(dt, B, T, N, chunk);
+    at::Tensor ws = workspace(wsb, x);
+    check_status(lpc_b200_backward_checkpointed(dt, gyc.data_ptr(), c.t.data_ptr(), ptr_or_null(zi),
+                                                xc.data_ptr(), sc.data_ptr(), gx.data_ptr(), ptr_or_null(gA),
+                                                ptr_or_null(gzi), B, T, N, c.sb, c.st, chunk, ptr_or_null(ws), wsb,
+                                                c10::cuda::getCurrentCUDAStream().stream()),
+                 "lpc_backward_checkpointed");
+    if (!need_A) gA = at::empty({0}, x.options());
+    if (!need_zi) gzi = at::empty({0}, x.options());
+    return {gx, gA, gzi};
+}
+
+// The error word: optionally synchronise the current stream, return the word
+// and clear it.
+int64_t check_status_op(bool synchronize) {
+    if (synchronize) c10::cuda::getCurrentCUDAStream().synchronize();
+    return (int64_t)take_error_word();
+}
+
+// Runs the library's bounded-wait self-test (a chunked forward whose
+// look-back waits for a flag nothing sets, given up after spin_limit polls)
+// with a workspace from the caching allocator on `like`'s device; returns the
+// C status (LPC_ERR_TIMEOUT when the wait gave up as designed).  The give-up
+// also reaches the error word, as any other would.
+int64_t selftest_timeout_op(const at::Tensor &like, int64_t spin_limit) {
+    check_cuda(like, "like");
+    ensure_error_word();
+    const c10::cuda::CUDAGuard guard(like.device());
+    const size_t wsb = lpc_b200_selftest_workspace_size();
+    at::Tensor ws = at::empty({(int64_t)wsb}, like.options().dtype(at::kByte));
+    unsigned st = 0;
+    return lpc_b200_selftest_timeout(ws.data_ptr(), wsb, (unsigned)spin_limit, &st,
+                                     c10::cuda::getCurrentCUDAStream().stream());
+}
+
 at::Tensor cpu_refused_ragged(const at::Tensor &, const at::Tensor &, const at::Tensor &,
                               const c10::optional<at::Tensor> &) {
     TORCH_CHECK(false, "torchlpc_b200 runs on CUDA devices only (no CPU implementation)");
@@ -297,6 +438,11 @@ TORCH_LIBRARY(torchlpc_b200, m) {
     m.def("lpc_ragged(Tensor x, Tensor A, Tensor offsets, Tensor? zi) -> Tensor");
     m.def("lpc_backward_ragged(Tensor grad_y, Tensor A, Tensor offsets, Tensor? zi, Tensor y, bool need_A, "
           "bool need_zi) -> (Tensor, Tensor, Tensor)");
+    m.def("lpc_checkpointed(Tensor x, Tensor A, Tensor? zi, int chunk) -> (Tensor, Tensor)");
+    m.def("lpc_backward_checkpointed(Tensor grad_y, Tensor A, Tensor? zi, Tensor x, Tensor states, int chunk, "
+          "bool need_A, bool need_zi) -> (Tensor, Tensor, Tensor)");
+    m.def("check_status(bool synchronize) -> int", &check_status_op);
+    m.def("selftest_timeout(Tensor like, int spin_limit) -> int");
     m.def("scan(Tensor input, Tensor weights, Tensor? initials, int algo=0) -> Tensor");
     m.def("scan_backward(Tensor grad_out, Tensor decay, Tensor? init, Tensor out, bool need_decay, "
           "bool need_init, int algo=0) -> (Tensor, Tensor, Tensor)");
@@ -309,6 +455,9 @@ TORCH_LIBRARY_IMPL(torchlpc_b200, CUDA, m) {
     m.impl("scan_backward", &scan_backward);
     m.impl("lpc_ragged", &lpc_ragged);
     m.impl("lpc_backward_ragged", &lpc_backward_ragged);
+    m.impl("lpc_checkpointed", &lpc_checkpointed);
+    m.impl("lpc_backward_checkpointed", &lpc_backward_checkpointed);
+    m.impl("selftest_timeout", &selftest_timeout_op);
 }
 
 TORCH_LIBRARY_IMPL(torchlpc_b200, CPU, m) {

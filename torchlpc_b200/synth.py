@@ -56,7 +56,8 @@ WORKLOADS = {
     "cfg2": Workload("cfg2", 64, 16000, 11, 80, 0.7, 0.98, 0.1,
                      note="analysis-by-synthesis frame rate, B=64 T=16000 N=22"),
     "cfg3": Workload("cfg3", 8, 1 << 20, 8, 512, 0.9, 0.999, 1.0,
-                     note="long-sequence chunked scan, B=8 T=2^20 N=16"),
+                     note="long-sequence chunked scan, B=8 T=2^20 N=16, fwd+bwd with boundary-state "
+                          "checkpointing"),
     "cfg4": Workload("cfg4", 1024, 0, 12, 160, 0.6, 0.99, 0.1, ragged=True,
                      note="ragged batch, 1024 signals, lengths log-uniform in [1024, 262144], N=24"),
     "cfg5": Workload("cfg5", 2048, 65536, 16, 0, 0.5, 0.95, 0.0, time_invariant=True,
