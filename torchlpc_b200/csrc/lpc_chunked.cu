@@ -169,12 +169,20 @@ __host__ __device__ constexpr int window_steps(int NP) {
     return (NP <= 16 ? 2 : 1) * NP * ((16 + NP - 1) / NP);
 }
 __host__ __device__ constexpr int ctas_per_sm(int NP, int esz) { return esz == 4 && NP > 16 ? 3 : 2; }
+// Phase-D (exact pass) windows: half the phase-A window, in fix_stages
+// stages (loads issued fix_stages - 1 windows ahead).  Measured on B200 at
+// order 16: quarter-length windows in four stages (the same shared memory)
+// made the pass 1.45x slower; its time follows the number of windows, not
+// the distance the loads run ahead.
+__host__ __device__ constexpr int fix_window(int NP) { return window_steps(NP) / 2; }
+__host__ __device__ constexpr int fix_stages(int) { return 2; }
 
 template <int NP>
 struct Cfg {
     static constexpr int THREADS = 256;
-    static constexpr int W = window_steps(NP);           // phase-A window: steps, a multiple of NP
-    static constexpr int WD = W / 2;                     // phase-D window (half-chunks, half the steps)
+    static constexpr int W = window_steps(NP);  // phase-A window: steps, a multiple of NP
+    static constexpr int WD = fix_window(NP);   // phase-D window (half-chunks)
+    static constexpr int DS = fix_stages(NP);   // phase-D stages in flight
 };
 
 // Per-chunk stride of a coefficient window in shared memory: WC rows of NP
@@ -259,11 +267,11 @@ struct SmemPlan {
     size_t abuf, ibuf, obuf, ybuf, maps, half, st, sin, lbP, lbz, misc, total;
     __host__ __device__ SmemPlan(size_t esz, int NP, int G, bool rev) {
         auto al = [](size_t v) { return (v + 15) & ~size_t(15); };
-        const int W = window_steps(NP), WD = W / 2;
+        const int W = window_steps(NP), WD = fix_window(NP), DS = fix_stages(NP);
         size_t off = 0;
         abuf = off;
         const size_t awin = al((size_t)2 * G * group_stride(W, NP, (int)esz) * esz);
-        const size_t dwin = al((size_t)2 * 2 * G * group_stride(WD, NP, (int)esz) * esz);
+        const size_t dwin = al((size_t)DS * 2 * G * group_stride(WD, NP, (int)esz) * esz);
         int Gp = 1;
         while (Gp < G) Gp <<= 1;
         const size_t mapbytes = al((size_t)Gp * map_stride(NP, (int)esz) * esz);
@@ -277,12 +285,12 @@ struct SmemPlan {
         if (awin > r) r = awin;
         if (dwin > r) r = dwin;
         off += al(r);
-        ibuf = off;  // inputs: 2 stages x G x W (= 2 stages x 2G x WD)
+        ibuf = off;  // inputs: 2 stages x G x W (= DS stages x 2G x WD: DS = 2, WD = W / 2)
         off += al((size_t)2 * G * W * esz);
         obuf = off;  // phase-D outputs of one window
         off += al((size_t)2 * G * WD * esz);
         ybuf = off;  // backward: lagged outputs y of the phase-D windows
-        if (rev) off += al((size_t)2 * 2 * G * (WD + NP) * esz);
+        if (rev) off += al((size_t)DS * 2 * G * (WD + NP) * esz);
         half = off;  // map over the first half of each chunk
         off += al((size_t)G * half_map_elems(NP, (int)esz) * esz);
         st = off;  // FP64 entry states of the tree nodes
@@ -333,7 +341,7 @@ struct Loader {
     // vectors l, l+32, ...  Inputs and lagged outputs follow on the low lanes.
     // The caller commits the group.
     __device__ static void load_vec(const ChunkParams<T> &p, const Sig &sg, int64_t tb, int Gc, int Lc, int w,
-                                    T *As, T *xs, T *ys, bool with_y) {
+                                    T *As, T *xs, T *ys, bool with_y, int lw0, int nlw) {
         constexpr int V = 16 / sizeof(T);
         constexpr int RV = NP / V > 0 ? NP / V : 1;  // vectors per row
         constexpr int AV = WC * RV;                  // coefficient vectors per chunk window
@@ -347,7 +355,7 @@ struct Loader {
         const T *Ab = p.A + sg.ao;
         const T *inb = p.in + sg.xo;
         const VT zero = {};
-        for (int g = threadIdx.x >> 5; g < Gc; g += NWARP) {
+        for (int g = (int)(threadIdx.x >> 5) - lw0; g < Gc; g += nlw) {
             int64_t row0;
             int lo, hi;
             rows(sg, tb, Lc, g, w, row0, lo, hi);
@@ -400,14 +408,14 @@ struct Loader {
     // Element path (any stride and alignment): one warp per chunk, one
     // cp.async per element.  The caller commits the group.
     __device__ static void load_elem(const ChunkParams<T> &p, const Sig &sg, int64_t tb, int Gc, int Lc, int w,
-                                     T *As, T *xs, T *ys, bool with_y, bool rows_too) {
+                                     T *As, T *xs, T *ys, bool with_y, bool rows_too, int lw0, int nlw) {
         constexpr int NWARP = THREADS / 32;
         const int N = p.N;
         const int lane = threadIdx.x & 31;
         const T *Ab = p.A + sg.ao;
         const T *inb = p.in + sg.xo;
         const T *zib = p.zi ? p.zi + sg.zo : nullptr;
-        for (int g = threadIdx.x >> 5; g < Gc; g += NWARP) {
+        for (int g = (int)(threadIdx.x >> 5) - lw0; g < Gc; g += nlw) {
             int64_t row0;
             int lo, hi;
             rows(sg, tb, Lc, g, w, row0, lo, hi);
@@ -451,16 +459,23 @@ struct Loader {
     }
 
     // Vector rows and inputs when both allow it; vector rows with element
-    // inputs when only the signal start or length is unaligned.
+    // inputs when only the signal start or length is unaligned.  Called by
+    // warps lw0 .. lw0+nlw-1 (every warp of the CTA by default), which share
+    // the chunks among them; PART false fixes them at compile time (every
+    // warp), which keeps the index arithmetic out of the registers of the
+    // large-order instances.
+    template <bool PART = false>
     __device__ static void load(const ChunkParams<T> &p, const Sig &sg, int64_t tb, int Gc, int Lc, int w, T *As,
-                                T *xs, T *ys, bool with_y) {
+                                T *xs, T *ys, bool with_y, int lw0_ = 0, int nlw_ = THREADS / 32) {
+        const int lw0 = PART ? lw0_ : 0;
+        const int nlw = PART ? nlw_ : THREADS / 32;
         if (p.loader == kLoadVec && sg.vx) {
-            load_vec(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y);
+            load_vec(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y, lw0, nlw);
         } else if (p.loader == kLoadVec) {
-            load_vec(p, sg, tb, Gc, Lc, w, As, nullptr, nullptr, false);
-            load_elem(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y, false);
+            load_vec(p, sg, tb, Gc, Lc, w, As, nullptr, nullptr, false, lw0, nlw);
+            load_elem(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y, false, lw0, nlw);
         } else {
-            load_elem(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y, true);
+            load_elem(p, sg, tb, Gc, Lc, w, As, xs, ys, with_y, true, lw0, nlw);
         }
     }
 };
@@ -554,6 +569,7 @@ template <typename T, int NP, bool REV, bool NEG>
 __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_kernel(ChunkParams<T> p) {
     constexpr int W = Cfg<NP>::W;
     constexpr int WD = Cfg<NP>::WD;
+    constexpr int DS = Cfg<NP>::DS;
     constexpr int THREADS = Cfg<NP>::THREADS;
     constexpr int V = 16 / sizeof(T);
     constexpr int GSA = group_stride(W, NP, sizeof(T));
@@ -595,7 +611,9 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
     const int TPC = (N + KF) / KF;  // phase-A lanes per chunk: N+1 filters, KF per lane
     const int grp = tid / TPC;
     const int kk = tid - grp * TPC;  // lane kk runs filters kk*KF .. kk*KF+KF-1
-    const int nwin = L / W;  // windows per pass (phase D: the same count of WD-step windows)
+    const int warp = tid >> 5;
+    const int aw = (G * TPC + 31) / 32;  // warps holding phase-A lanes
+    const int nwin = L / W;  // phase-A windows per chunk
     const int64_t nbatches = p.roff ? p.bb[p.nsig] : p.nbatches;
     Sig *sgs = reinterpret_cast<Sig *>(misc + 1);
 
@@ -686,31 +704,64 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
             for (int j = 0; j < NP; ++j) h[q][j] = (active && f < N && j == state_slot<REV, NP>(f)) ? T(1) : T(0);
         }
         if (!p.fixonly) {
-            LA::load(p, sg, tb, Gb, L, 0, Abuf, ibuf, nullptr, false);
-            cp_async_commit();
-            for (int w = 0; w < nwin; ++w) {
-                const int s = w & 1;
-                if (w + 1 < nwin)
-                    LA::load(p, sg, tb, Gb, L, w + 1, Abuf + (size_t)(s ^ 1) * G * GSA,
-                             ibuf + (size_t)(s ^ 1) * G * W, nullptr, false);
+            if constexpr (NP <= 16) {
+                // Warps that hold no phase-A lane (aw .. 7) issue the next
+                // window's loads while the others compute this one (one
+                // barrier per window; measured 6 % faster at order 16 on
+                // B200).
+                // (the plan leaves at least one such warp at these orders)
+                const bool lwarp = warp >= aw;
+                const int nlw = THREADS / 32 - aw;
+                if (lwarp) LA::template load<true>(p, sg, tb, Gb, L, 0, Abuf, ibuf, nullptr, false, aw, nlw);
                 cp_async_commit();
-                cp_async_wait<1>();
-                __syncthreads();
-                if (active) {
-                    if (w == nwin / 2) {
-                        // the state after the first half of the chunk (in scan
-                        // order): the lane's columns of the half map (or its z)
+                for (int w = 0; w < nwin; ++w) {
+                    const int s = w & 1;
+                    cp_async_wait<0>();  // window w (issued by this thread, if a loader)
+                    __syncthreads();     // window w is visible, window w-1's stage is free
+                    if (lwarp && w + 1 < nwin)
+                        LA::template load<true>(p, sg, tb, Gb, L, w + 1, Abuf + (size_t)(s ^ 1) * G * GSA,
+                                                ibuf + (size_t)(s ^ 1) * G * W, nullptr, false, aw, nlw);
+                    cp_async_commit();
+                    if (active) {
+                        if (w == nwin / 2) {
 #pragma unroll
-                        for (int q = 0; q < KF; ++q)
-                            put_map_column<T, NP, REV>(hmap + (size_t)grp * HME, NP, h[q], kk * KF + q, N);
-                    }
-                    const T *Ag = Abuf + (size_t)s * G * GSA + (size_t)grp * GSA;
-                    const T *xg = ibuf + (size_t)s * G * W + (size_t)grp * W;
+                            for (int q = 0; q < KF; ++q)
+                                put_map_column<T, NP, REV>(hmap + (size_t)grp * HME, NP, h[q], kk * KF + q, N);
+                        }
+                        const T *Ag = Abuf + (size_t)s * G * GSA + (size_t)grp * GSA;
+                        const T *xg = ibuf + (size_t)s * G * W + (size_t)grp * W;
 #pragma unroll 1
-                    for (int blk = 0; blk < W / NP; ++blk)
-                        map_steps<T, NP, KF, REV, NEG, W, 0, NP>(Ag, xg, xmask, blk * NP, h);
+                        for (int blk = 0; blk < W / NP; ++blk)
+                            map_steps<T, NP, KF, REV, NEG, W, 0, NP>(Ag, xg, xmask, blk * NP, h);
+                    }
                 }
-                __syncthreads();
+            } else {
+                LA::load(p, sg, tb, Gb, L, 0, Abuf, ibuf, nullptr, false);
+                cp_async_commit();
+                for (int w = 0; w < nwin; ++w) {
+                    const int s = w & 1;
+                    if (w + 1 < nwin)
+                        LA::load(p, sg, tb, Gb, L, w + 1, Abuf + (size_t)(s ^ 1) * G * GSA,
+                                 ibuf + (size_t)(s ^ 1) * G * W, nullptr, false);
+                    cp_async_commit();
+                    cp_async_wait<1>();
+                    __syncthreads();
+                    if (active) {
+                        if (w == nwin / 2) {
+                            // the state after the first half of the chunk (in scan
+                            // order): the lane's columns of the half map (or its z)
+#pragma unroll
+                            for (int q = 0; q < KF; ++q)
+                                put_map_column<T, NP, REV>(hmap + (size_t)grp * HME, NP, h[q], kk * KF + q, N);
+                        }
+                        const T *Ag = Abuf + (size_t)s * G * GSA + (size_t)grp * GSA;
+                        const T *xg = ibuf + (size_t)s * G * W + (size_t)grp * W;
+#pragma unroll 1
+                        for (int blk = 0; blk < W / NP; ++blk)
+                            map_steps<T, NP, KF, REV, NEG, W, 0, NP>(Ag, xg, xmask, blk * NP, h);
+                    }
+                    __syncthreads();
+                }
             }
             cp_async_wait<0>();
             __syncthreads();
@@ -954,7 +1005,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
         // starts each half-chunk from the recorded one.
         const int Gd = 2 * Gb;  // half-chunks of the batch
         if (p.loader == kLoadElem && N < NP)
-            for (int e = tid; e < 2 * 2 * G * GSD; e += THREADS)
+            for (int e = tid; e < DS * 2 * G * GSD; e += THREADS)
                 if ((e % GSD) % NP >= N) Abuf[e] = T(0);
         const bool fix = tid < Gd;
         {
@@ -990,6 +1041,12 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_ke
         // grad_A rows are dense (B,T,N): 16-byte vectors when N fills NP
         const bool gA_vec = N == NP && NP % V == 0 && is_aligned16<T>(p.gA);
         __syncthreads();
+        // Every warp loads the next window, then the phase-D lanes compute
+        // (leaving the loads to the warps without phase-D lanes, as phase A
+        // does, measured 10 % slower in the backward: those loads are the
+        // larger part of the window's time there).  nwin windows of WD steps
+        // cover a half-chunk.
+        static_assert(DS == 2 && 2 * WD == W, "phase D is double buffered, half-length windows");
         LD::load(p, sg, tb, Gd, LH, 0, Abuf, ibuf, ybuf, REV);
         cp_async_commit();
         for (int w = 0; w < nwin; ++w) {
@@ -1128,6 +1185,10 @@ inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N, int64_t dflt 
     const int Gk = (int)(threads_for(pl.NP) / ((N + KF) / KF));
     if (Gk > G) G = Gk < 16 ? Gk : (G > 16 ? G : 16);
     if (G > kMaxChunksPerBatch) G = kMaxChunksPerBatch;
+    // orders up to 16 keep at least one warp free of phase-A lanes: it loads
+    // the next window while the others compute
+    if (pl.NP <= 16)
+        while (G > 1 && G * ((N + KF) / KF) > threads_for(pl.NP) - 32) --G;
     const int ctas = ctas_per_sm(pl.NP, (int)esz);
     const size_t budget = (size_t)228 * 1024 / ctas - 1024;  // per-SM shared memory less the per-CTA reserve
     while (G > 1 && SmemPlan(esz, pl.NP, G, true).total > budget) --G;

@@ -44,11 +44,21 @@ __device__ __forceinline__ void warp_copy_async(T *dst, const T *src, int count,
 
 template <typename T, int NP>
 __device__ __forceinline__ T hist_dot(const T *a, const T (&h)[NP], int u_minus_1, T acc) {
-    // acc - sum_i a[i] * h[(u-1-i) mod NP], oldest tap first so that the
-    // newest history value enters last (one FMA on the loop-carried path).
+    // acc - sum_i a[i] * h[(u-1-i) mod NP].  The older taps go into four
+    // independent partial sums (short chains that overlap the previous step)
+    // and the newest history value enters last, so the loop-carried path of
+    // the recurrence is one FMA.
+    if constexpr (NP < 4) {
 #pragma unroll
-    for (int i = NP - 1; i >= 0; --i) acc = fma(-a[i], h[(u_minus_1 - i + 2 * NP) % NP], acc);
-    return acc;
+        for (int i = NP - 1; i >= 0; --i) acc = fma(-a[i], h[(u_minus_1 - i + 2 * NP) % NP], acc);
+        return acc;
+    } else {
+        T ps[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+        for (int i = NP - 1; i >= 1; --i) ps[i & 3] = fma(a[i], h[(u_minus_1 - i + 2 * NP) % NP], ps[i & 3]);
+        acc = acc - ((ps[0] + ps[1]) + (ps[2] + ps[3]));
+        return fma(-a[0], h[(u_minus_1 + 2 * NP) % NP], acc);
+    }
 }
 
 template <typename T, int NP, int R>
@@ -256,14 +266,18 @@ __global__ void __launch_bounds__(32 * kPlainWarps) bwd_plain_kernel(BwdArgs<T> 
             if (t_hi >= t_lo) {
                 const T sgn = NEG ? T(1) : T(-1);
                 if (!ti) {
-                    const int64_t cnt = (t_hi - t_lo + 1) * N;
+                    // a row of N taps per step, lanes along the row (coalesced;
+                    // 32-bit indices within the batch, no division per element)
+                    const int nrow = (int)(t_hi - t_lo + 1);
                     T *gAb = p.gA + (b * Tn + t_lo) * N;
-                    for (int64_t e = lane; e < cnt; e += 32) {
-                        const int64_t t = t_lo + e / N;
-                        const int i = (int)(e - (t - t_lo) * N);
-                        const int64_t j = t - 1 - i;
-                        const T yv = j >= 0 ? yb[j] : (zib ? zib[-1 - j] : T(0));
-                        gAb[e] = sgn * gxbuf[t_first - t] * yv;
+                    for (int rr = 0; rr < nrow; ++rr) {
+                        const int64_t t = t_lo + rr;
+                        const T g = sgn * gxbuf[t_first - t];
+                        for (int i = lane; i < N; i += 32) {
+                            const int64_t j = t - 1 - i;
+                            const T yv = j >= 0 ? yb[j] : (zib ? zib[-1 - j] : T(0));
+                            gAb[rr * N + i] = g * yv;
+                        }
                     }
                 } else if (lane < N) {
                     for (int64_t t = t_lo; t <= t_hi; ++t) {
