@@ -141,20 +141,25 @@ __global__ void __launch_bounds__(32 * kPlainWarps) fwd_plain_kernel(FwdArgs<T> 
         if (lane == 0) {
             const T *As = Abuf + (k & 1) * R * NP;
             const T *xs = xbuf + (k & 1) * R;
+            // the next step's coefficient row is read while this step's
+            // dot product runs (the shared-memory latency stays off the chain)
+            T a[NP];
+            load_row_vec<T, NP, R>(a, As);
 #pragma unroll 1
             for (int blk = 0; blk < R / NP; ++blk) {
 #pragma unroll
                 for (int u = 0; u < NP; ++u) {
                     const int r = blk * NP + u;
-                    T a[NP];
-                    load_row_vec<T, NP, R>(a, As + r * NP);
-                    if constexpr (NEG) {
+                    T an[NP] = {};
+                    if (r + 1 < R) load_row_vec<T, NP, R>(an, As + (r + 1) * NP);
+                    T ac[NP];
 #pragma unroll
-                        for (int i = 0; i < NP; ++i) a[i] = -a[i];
-                    }
-                    const T v = hist_dot<T, NP>(a, h, u - 1, xs[r]);
+                    for (int i = 0; i < NP; ++i) ac[i] = NEG ? -a[i] : a[i];
+                    const T v = hist_dot<T, NP>(ac, h, u - 1, xs[r]);
                     h[u] = v;
                     ybuf[r] = v;
+#pragma unroll
+                    for (int i = 0; i < NP; ++i) a[i] = an[i];
                 }
             }
         }
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(32 * kPlainWarps) fwd_plain_kernel(FwdArgs<T> 
 template <typename T, int NP, bool NEG>
 __global__ void __launch_bounds__(32 * kPlainWarps) bwd_plain_kernel(BwdArgs<T> p) {
     constexpr int R = plain_rows(NP);
-    constexpr int PER_WARP = 2 * R * NP + 3 * R;
+    constexpr int PER_WARP = 2 * R * NP + 3 * R + 2 * (R + NP);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = (int64_t)blockIdx.x * kPlainWarps + warp;
@@ -182,6 +187,7 @@ __global__ void __launch_bounds__(32 * kPlainWarps) bwd_plain_kernel(BwdArgs<T> 
     T *Dbuf = reinterpret_cast<T *>(smem_raw) + warp * PER_WARP;  // skewed diagonal
     T *gbuf = Dbuf + 2 * R * NP;
     T *gxbuf = gbuf + 2 * R;
+    T *ybuf = gxbuf + R;  // 2 stages of the R + NP outputs y the batch's grad_A needs
     const T *Ab = p.A + b * p.a_stride_b;
     const T *gyb = p.gy + b * Tn;
     const T *yb = p.y + b * Tn;
@@ -217,6 +223,20 @@ __global__ void __launch_bounds__(32 * kPlainWarps) bwd_plain_kernel(BwdArgs<T> 
         const int64_t t_first = top - 1;  // slot 0
         const int nvalid = (int)max64(0, min64(R, t_first + 1));
         for (int s = lane; s < nvalid; s += 32) cp_async<sizeof(T)>(gs + s, gyb + (t_first - s));
+        // y[j] for j = jbase .. jbase+R+NP-1 (zi before the signal), so that
+        // the grad_A epilogue reads shared memory instead of waiting on a
+        // global load per row
+        if (p.gA && !ti) {
+            T *ys = ybuf + (k & 1) * (R + NP);
+            const int64_t jbase = t_first - R + 1 - NP;
+            for (int m = lane; m < R + NP; m += 32) {
+                const int64_t j = jbase + m;
+                if (j >= 0)
+                    cp_async<sizeof(T)>(ys + m, yb + j);
+                else
+                    ys[m] = (zib && -1 - j < N) ? zib[-1 - j] : T(0);
+            }
+        }
     };
 
     T h[NP];
@@ -234,20 +254,23 @@ __global__ void __launch_bounds__(32 * kPlainWarps) bwd_plain_kernel(BwdArgs<T> 
         if (lane == 0) {
             const T *Ds = Dbuf + (k & 1) * R * NP;
             const T *gs = gbuf + (k & 1) * R;
+            T a[NP];
+            load_row_vec<T, NP, R>(a, Ds);
 #pragma unroll 1
             for (int blk = 0; blk < R / NP; ++blk) {
 #pragma unroll
                 for (int u = 0; u < NP; ++u) {
                     const int s = blk * NP + u;
-                    T a[NP];
-                    load_row_vec<T, NP, R>(a, Ds + s * NP);
-                    if constexpr (NEG) {
+                    T an[NP] = {};
+                    if (s + 1 < R) load_row_vec<T, NP, R>(an, Ds + (s + 1) * NP);
+                    T ac[NP];
 #pragma unroll
-                        for (int i = 0; i < NP; ++i) a[i] = -a[i];
-                    }
-                    const T v = hist_dot<T, NP>(a, h, u - 1, gs[s]);
+                    for (int i = 0; i < NP; ++i) ac[i] = NEG ? -a[i] : a[i];
+                    const T v = hist_dot<T, NP>(ac, h, u - 1, gs[s]);
                     h[u] = v;
                     gxbuf[s] = v;
+#pragma unroll
+                    for (int i = 0; i < NP; ++i) a[i] = an[i];
                 }
             }
         }
@@ -270,14 +293,13 @@ __global__ void __launch_bounds__(32 * kPlainWarps) bwd_plain_kernel(BwdArgs<T> 
                     // 32-bit indices within the batch, no division per element)
                     const int nrow = (int)(t_hi - t_lo + 1);
                     T *gAb = p.gA + (b * Tn + t_lo) * N;
+                    const T *ys = ybuf + (k & 1) * (R + NP);
+                    const int64_t jbase = t_first - R + 1 - NP;
                     for (int rr = 0; rr < nrow; ++rr) {
                         const int64_t t = t_lo + rr;
                         const T g = sgn * gxbuf[t_first - t];
-                        for (int i = lane; i < N; i += 32) {
-                            const int64_t j = t - 1 - i;
-                            const T yv = j >= 0 ? yb[j] : (zib ? zib[-1 - j] : T(0));
-                            gAb[rr * N + i] = g * yv;
-                        }
+                        const T *yr = ys + (int)(t - 1 - jbase);  // y[t-1-i] = yr[-i]
+                        for (int i = lane; i < N; i += 32) gAb[rr * N + i] = g * yr[-i];
                     }
                 } else if (lane < N) {
                     for (int64_t t = t_lo; t <= t_hi; ++t) {
@@ -408,7 +430,7 @@ static cudaError_t launch_fwd_np(const FwdArgs<T> &p, cudaStream_t st) {
 template <typename T, int NP, bool NEG>
 static cudaError_t launch_bwd_np(const BwdArgs<T> &p, cudaStream_t st) {
     constexpr int R = plain_rows(NP);
-    const size_t smem = (size_t)kPlainWarps * (2 * R * NP + 3 * R) * sizeof(T);
+    const size_t smem = (size_t)kPlainWarps * (2 * R * NP + 3 * R + 2 * (R + NP)) * sizeof(T);
     auto kern = bwd_plain_kernel<T, NP, NEG>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
