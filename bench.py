@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda-probe"])
     ap.add_argument("--config", default="cfg3", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
     ap.add_argument("--algo", default="auto", choices=["auto", "plain", "chunked"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -498,6 +498,69 @@ def run_reference(args):
     return 0
 
 
+# --------------------------------------------------------------------------- reference CUDA kernels
+REF_CUDA_T = 1 << 15  # samples per signal of the bounded sample the reference CUDA kernels are timed on
+
+
+def run_reference_cuda_probe(args):
+    """The reference's own CUDA path (torchlpc/csrc/cuda/lpc.cu and its
+    autograd backward, built unmodified for sm_100a into oracle/_ref_cuda) on
+    a bounded sample of the workload: all B signals, the first REF_CUDA_T
+    samples.  Runs in its own process (it registers the torchlpc op
+    namespace); prints one JSON line."""
+    from oracle.build import build_reference_cuda
+
+    path = build_reference_cuda()
+    if path is None:
+        print(json.dumps({"unavailable": "reference CUDA build (oracle/_ref_cuda) missing"}))
+        return 0
+    sys.path.insert(0, str(path))
+    import warnings
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        import torchlpc
+    if not torchlpc.EXTENSION_LOADED:
+        print(json.dumps({"unavailable": "reference CUDA extension failed to load"}))
+        return 0
+    T = min(REF_CUDA_T, args.T) if args.T else REF_CUDA_T
+    w = load_workload(args.config, "cpu", T=T)
+    if w["workload"].ragged:
+        print(json.dumps({"unavailable": "no ragged API in the reference"}))
+        return 0
+    dev = "cuda"
+    x, A, zi, gy = (w[k].to(dev) for k in ("x", "A", "zi", "gy"))
+
+    def step():
+        xx, AA, zz = (t.clone().requires_grad_(True) for t in (x, A, zi))
+        Ae = AA[:, None, :].expand(-1, w["T"], -1) if w["workload"].time_invariant else AA
+        y = torchlpc.sample_wise_lpc(xx, Ae, zz)
+        y.backward(gy)
+
+    ms = time_loop(step, max(1, args.steps), max(1, args.warmup), torch.device(dev))
+    S = samples_of(w)
+    print(json.dumps({"value": S / (ms * 1e-3), "unit": "samples/s", "ms_per_step": ms,
+                      "sample": f"{w['B']} signals x T={w['T']} (first samples of the workload's shapes)",
+                      "path": "reference torchlpc CUDA kernel lpc.cu (one block per signal) + its autograd "
+                              "backward, built unmodified for sm_100a"}))
+    return 0
+
+
+def reference_cuda_line(args):
+    """Run the probe above in a child process; returns its JSON or an
+    'unavailable' record."""
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference-cuda-probe", "--config", args.config,
+           "--steps", "3", "--warmup", "1"]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        for line in reversed(r.stdout.strip().splitlines()):
+            if line.startswith("{"):
+                return json.loads(line)
+        return {"unavailable": f"probe exited {r.returncode}: {r.stderr.strip().splitlines()[-1:]}"}
+    except (subprocess.TimeoutExpired, OSError, ValueError) as e:
+        return {"unavailable": f"probe failed: {e}"}
+
+
 def other_configs(tl, headline: str, device) -> dict:
     """fwd+bwd samples/s of the other workloads at their full sizes (operator
     level, CUDA events; the default algorithm, and the plain kernel where it
@@ -575,34 +638,49 @@ def run_ours(args):
         line["clocks"] = clocks
 
     if rk == 0:
-        # roofline of the dominant kernel (forward or fused backward operator)
+        # roofline of the dominant kernel: the forward and the fused backward
+        # kernels timed alone (the saved-y operators, one launch each; the
+        # checkpointed backward operator adds the exact-pass recompute of y)
         tf, tb = kernel_times(tl, w, x, A, zi, gy, max(5, args.steps // 2), device, ckpt=ckpt)
+        if ckpt:
+            tkf, tkb = kernel_times(tl, w, x, A, zi, gy, max(5, args.steps // 2), device, ckpt=False)
+        else:
+            tkf, tkb = tf, tb
         peak, peak_kind = measured_peaks()
         bf, bb = bytes_per_sample(w["N"], wl.time_invariant)
-        kern, t_k, b_k = ("backward", tb, bb) if tb >= tf else ("forward", tf, bf)
+        kern, t_k, b_k = ("backward", tkb, bb) if tkb >= tkf else ("forward", tkf, bf)
         achieved = S * b_k / (t_k * 1e-3) / 1e9
         tr = traffic_from_profiles(args.config, kern)
-        line["roofline"] = {"bound": "hbm", "kernel": f"fused {kern} operator", "achieved": achieved,
+        line["roofline"] = {"bound": "hbm", "kernel": f"fused {kern} kernel (chunked scan)", "achieved": achieved,
                             "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                             "peak_source": peak_kind, "traffic": tr,
-                            "algorithmic_bytes_per_launch": S * b_k, "launch_ms": t_k}
+                            "algorithmic_bytes_per_launch": S * b_k, "launch_ms": t_k,
+                            "bytes_per_sample": {"forward": bf, "backward": bb},
+                            "kernel_frac": {"forward": S * bf / (tkf * 1e-3) / 1e9 / peak,
+                                            "backward": S * bb / (tkb * 1e-3) / 1e9 / peak}}
         step_bytes = S * (bf + bb)
         line["hbm_frac_fwd_bwd"] = step_bytes / (ms * 1e-3) / 1e9 / peak
         line["kernel_ms"] = {"forward": tf, "backward": tb}
+        if ckpt:
+            line["kernel_ms"]["backward_kernel"] = tkb
+            line["kernel_ms"]["recompute_pass"] = tb - tkb
         if ckpt:
             # the same step keeping y for the backward instead of the states
             old = tl.get_checkpointing()
             tl.set_checkpointing("off")
             mss = time_loop(step, args.steps, 3, device)
-            tsf, tsb = kernel_times(tl, w, x, A, zi, gy, max(5, args.steps // 2), device, ckpt=False)
             tl.set_checkpointing(old)
             line["saved_y"] = {"value": S / (mss * 1e-3), "ms_per_step": mss,
-                               "kernel_ms": {"forward": tsf, "backward": tsb}}
+                               "kernel_ms": {"forward": tkf, "backward": tkb}}
         # scan vs plain on the same GPU
         if args.algo != "plain" and "chunked" in tl.available_algos():
             tl.set_algo("plain")
             msp = time_loop(step, max(2, args.steps // 4), 1, device)
             tl.set_algo(args.algo)
+            # the reference's own CUDA kernels on the same GPU (bounded sample)
+            line["reference_cuda"] = reference_cuda_line(args)
+            if "value" in line["reference_cuda"]:
+                line["reference_cuda"]["ours_over_reference_cuda"] = value / line["reference_cuda"]["value"]
             line["plain"] = {"value": S / (msp * 1e-3), "ms_per_step": msp,
                              "speedup": msp / ms}
         line["max_rel_err_vs_fp64"] = oracle_errors(tl, w, x, A, zi, gy)
@@ -635,6 +713,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.impl == "reference-cuda-probe":
+        return run_reference_cuda_probe(args)
     return run_ours(args)
 
 
