@@ -23,15 +23,9 @@ namespace lpcb {
 
 namespace {
 
-constexpr int kTiChunk = 1024;  // target chunk length, rounded to a multiple of the staged window
+constexpr int kTiChunk = 1024;  // target chunk length, rounded to a multiple of the padded order
 
-// Steps per staged window: whole turns of the history ring, near 32 steps
-// (a multiple of 4: whole 16-byte groups).
-__host__ __device__ constexpr int ti_window(int NP) { return NP * ((32 + NP - 1) / NP); }
-inline int ti_chunk_len(int NP) {
-    const int S = ti_window(NP);
-    return S * ((kTiChunk + S - 1) / S);
-}
+inline int ti_chunk_len(int NP) { return NP * ((kTiChunk + NP - 1) / NP); }
 inline size_t al256(size_t v) { return (v + 255) & ~size_t(255); }
 
 struct TiLayout {
@@ -244,124 +238,6 @@ __global__ void __launch_bounds__(256) ti_chunk_kernel(TiArgs<T> p) {
     }
 }
 
-// Staged variant (fp32, 16-byte rows): the NT streams of a CTA (one per
-// thread) move through shared memory in windows of S steps.  Every thread
-// copies 16-byte pieces of all the CTA's streams (8 consecutive threads take
-// one stream's 128 bytes: coalesced), one window ahead of the compute; each
-// thread then reads its own stream from its padded row (16-byte rows, rows 16
-// bytes apart modulo 128: conflict-free).  The plain kernel above gives each
-// thread one 16-byte group of lookahead, so every group waited out a DRAM
-// latency.
-constexpr int kTiThreads = 256;
-
-template <int NP>
-constexpr size_t ti_staged_smem(int nt, int streams) {
-    return (size_t)2 * streams * nt * (ti_window(NP) + 4) * sizeof(float) + (size_t)nt * (sizeof(int64_t) + sizeof(int));
-}
-
-// Copies window w of the CTA's streams into dst ([NT][S+4]).  sbase[i]: element
-// (row offset included) of window 0's first element of stream i; window w
-// starts S*w elements later (forward) or earlier (REV: steps run down the
-// row).  snst[i]: the stream's valid steps; pieces past them read zero.
-template <int NP, int NT, bool REV>
-__device__ __forceinline__ void ti_stage_window(const float *src, const int64_t *sbase, const int *snst, int w,
-                                                float *dst) {
-    constexpr int S = ti_window(NP);
-    constexpr int RW = S + 4;
-    constexpr int VS = S / 4;
-#pragma unroll
-    for (int k = 0; k < VS; ++k) {
-        const int v = (int)threadIdx.x + k * NT;
-        const int i = v / VS;
-        const int q = v - i * VS;
-        // steps [top-4, top) of the stream sit in piece q
-        const int top = REV ? w * S + S - 4 * q : w * S + 4 * q + 4;
-        float *d = dst + (size_t)i * RW + 4 * q;
-        if (top <= snst[i])
-            cp_async<16>(d, src + sbase[i] + (REV ? -(int64_t)w * S : (int64_t)w * S) + 4 * q);
-        else
-            *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-}
-
-template <int NP, bool REV, bool FIX>
-__global__ void __launch_bounds__(kTiThreads) ti_chunk_staged_kernel(TiArgs<float> p) {
-    constexpr int NT = kTiThreads;
-    constexpr int S = ti_window(NP);
-    constexpr int RW = S + 4;
-    extern __shared__ __align__(16) float tsm[];
-    float *win = tsm;  // [2][NT][RW]
-    int64_t *sbase = reinterpret_cast<int64_t *>(tsm + (size_t)2 * NT * RW);
-    int *snst = reinterpret_cast<int *>(sbase + NT);
-    const int tid = threadIdx.x;
-    const int64_t idx = (int64_t)blockIdx.x * NT + tid;
-    const bool on = idx < p.B * p.nc;
-    const int64_t b = on ? idx / p.nc : 0;
-    const int64_t c = on ? idx - b * p.nc : 0;
-    const int64_t s0 = c * p.Lc;
-    const int nst = on ? (int)(min64(s0 + p.Lc, p.T) - s0) : 0;
-    sbase[tid] = b * p.T + (REV ? p.T - s0 - S : s0);
-    snst[tid] = nst;
-    const int N = p.N;
-    float a[NP];
-#pragma unroll
-    for (int i = 0; i < NP; ++i) a[i] = (on && i < N) ? p.a[b * p.as_b + i] : 0.f;
-    float h[NP];
-    if constexpr (FIX) {
-        const float *e = p.est + (size_t)(on ? idx : 0) * NP;
-#pragma unroll
-        for (int i = 0; i < NP; ++i) h[ti_slot<NP>(i)] = on ? e[i] : 0.f;
-    } else {
-#pragma unroll
-        for (int i = 0; i < NP; ++i) h[i] = 0.f;
-    }
-    float *outb = p.out + b * p.T;
-    __syncthreads();
-    const int nwin = p.Lc / S;
-    ti_stage_window<NP, NT, REV>(p.in, sbase, snst, 0, win);
-    cp_async_commit();
-#pragma unroll 1
-    for (int w = 0; w < nwin; ++w) {
-        const int s = w & 1;
-        if (w + 1 < nwin) ti_stage_window<NP, NT, REV>(p.in, sbase, snst, w + 1, win + (size_t)(s ^ 1) * NT * RW);
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        const float4 *xr = reinterpret_cast<const float4 *>(win + (size_t)s * NT * RW + (size_t)tid * RW);
-#pragma unroll
-        for (int g = 0; g < S / 4; ++g) {
-            // steps 4g..4g+3 of the window: forward elements 4g.., backward S-1-4g..
-            const float4 q4 = xr[REV ? S / 4 - 1 - g : g];
-            const float xin[4] = {REV ? q4.w : q4.x, REV ? q4.z : q4.y, REV ? q4.y : q4.z, REV ? q4.x : q4.w};
-            float o[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int u = (4 * g + k) % NP;
-                h[u] = ti_step<float, NP>(a, h, u, xin[k]);
-                o[k] = h[u];
-            }
-            if constexpr (FIX) {
-                const int st = w * S + 4 * g;  // step of o[0] within the chunk
-                if (st < nst) {
-                    const int64_t t = REV ? p.T - 4 - (s0 + st) : s0 + st;
-                    *reinterpret_cast<float4 *>(outb + t) =
-                        REV ? make_float4(o[3], o[2], o[1], o[0]) : make_float4(o[0], o[1], o[2], o[3]);
-                }
-            }
-        }
-        __syncthreads();  // stage s is refilled next
-    }
-    cp_async_wait<0>();
-    if constexpr (!FIX) {
-        // exit state after the chunk (a partial last chunk has no successor)
-        if (on) {
-            float *z = p.zst + (size_t)idx * NP;
-#pragma unroll
-            for (int i = 0; i < NP; ++i) z[i] = h[ti_slot<NP>(i)];
-        }
-    }
-}
-
 // ---------------------------------------------------------------- combine
 // One warp per signal: lane r keeps row r of P; s_{c+1} = P s_c + z_c (FP64).
 // The zero-state exit states of 8 chunks are loaded ahead of the chain (a
@@ -482,99 +358,6 @@ __global__ void __launch_bounds__(256) ti_grad_a_kernel(const T *gx, const T *y,
     }
 }
 
-// Staged variant of the reduction (fp32, 16-byte rows): both streams of
-// every thread (grad_x and y over its segment) move through shared memory in
-// windows of S steps, copied one window ahead by the whole CTA as in
-// ti_chunk_staged_kernel.
-constexpr int kTiGradThreads = 128;
-
-template <int NP>
-__global__ void __launch_bounds__(kTiGradThreads) ti_grad_a_staged_kernel(const float *gx, const float *y,
-                                                                         const float *zi, float *ga, int64_t B,
-                                                                         int64_t T_, int N, int seg, int64_t nseg,
-                                                                         float sgn) {
-    constexpr int NT = kTiGradThreads;
-    constexpr int S = ti_window(NP);
-    constexpr int RW = S + 4;
-    extern __shared__ __align__(16) float tsm[];
-    float *gwin = tsm;                         // [2][NT][RW]
-    float *ywin = tsm + (size_t)2 * NT * RW;   // [2][NT][RW]
-    int64_t *sbase = reinterpret_cast<int64_t *>(tsm + (size_t)4 * NT * RW);
-    int *snst = reinterpret_cast<int *>(sbase + NT);
-    const int tid = threadIdx.x;
-    const int64_t idx = (int64_t)blockIdx.x * NT + tid;
-    const bool on = idx < B * nseg;
-    const int64_t b = on ? idx / nseg : -1;
-    const int64_t t0 = on ? (idx - b * nseg) * seg : 0;
-    const int nst = on ? (int)(min64(t0 + seg, T_) - t0) : 0;
-    sbase[tid] = (on ? b : 0) * T_ + t0;
-    snst[tid] = nst;
-    float acc[NP];
-#pragma unroll
-    for (int i = 0; i < NP; ++i) acc[i] = 0.f;
-    float yr[NP];
-    {
-        const float *yb = y + (on ? b : 0) * T_;
-        const float *zb = (on && zi) ? zi + b * N : nullptr;
-#pragma unroll
-        for (int i = 0; i < NP; ++i) {
-            const int64_t j = t0 - 1 - i;
-            yr[i] = !on ? 0.f : (j >= 0 ? yb[j] : ((zb && -1 - j < N) ? zb[-1 - j] : 0.f));
-        }
-    }
-    __syncthreads();
-    const int nwin = seg / S;
-    ti_stage_window<NP, NT, false>(gx, sbase, snst, 0, gwin);
-    ti_stage_window<NP, NT, false>(y, sbase, snst, 0, ywin);
-    cp_async_commit();
-#pragma unroll 1
-    for (int w = 0; w < nwin; ++w) {
-        const int s = w & 1;
-        if (w + 1 < nwin) {
-            ti_stage_window<NP, NT, false>(gx, sbase, snst, w + 1, gwin + (size_t)(s ^ 1) * NT * RW);
-            ti_stage_window<NP, NT, false>(y, sbase, snst, w + 1, ywin + (size_t)(s ^ 1) * NT * RW);
-        }
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        const float4 *gr = reinterpret_cast<const float4 *>(gwin + (size_t)s * NT * RW + (size_t)tid * RW);
-        const float4 *yq = reinterpret_cast<const float4 *>(ywin + (size_t)s * NT * RW + (size_t)tid * RW);
-#pragma unroll
-        for (int g = 0; g < S / 4; ++g) {
-            const float4 g4 = gr[g], y4 = yq[g];
-            const float gv[4] = {g4.x, g4.y, g4.z, g4.w};
-            const float yv[4] = {y4.x, y4.y, y4.z, y4.w};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int u = (4 * g + k) % NP;
-#pragma unroll
-                for (int i = 0; i < NP; ++i) acc[i] = fma(gv[k], yr[(i - u + NP) % NP], acc[i]);
-                yr[NP - 1 - u] = yv[k];
-            }
-        }
-        __syncthreads();  // stage s is refilled next
-    }
-    cp_async_wait<0>();
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    // every lane takes part in both collectives (idle lanes included)
-    const int64_t b0 = __shfl_sync(full, b, 0);
-    const bool uniform = __all_sync(full, on && b == b0);
-    if (uniform) {
-#pragma unroll
-        for (int i = 0; i < NP; ++i) {
-            float v = acc[i];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(full, v, o);
-            if (lane == 0 && i < N && v != 0.f) atomicAdd(ga + b * N + i, sgn * v);
-        }
-    } else if (on) {
-#pragma unroll
-        for (int i = 0; i < NP; ++i)
-            if (i < N && acc[i] != 0.f) atomicAdd(ga + b * N + i, sgn * acc[i]);
-    }
-}
-
 // grad_zi[b,k] = -sum_{i=k}^{N-1} a[b,i] grad_x[b,i-k]  (grad_x beyond T is 0)
 template <typename T>
 __global__ void ti_grad_zi_kernel(const T *gx, const T *a, int64_t as_b, T *gzi, int64_t B, int64_t T_, int N) {
@@ -595,31 +378,14 @@ cudaError_t ti_run(TiArgs<T> p, cudaStream_t st) {
     const unsigned g1 = (unsigned)((threads + 255) / 256);
     // 16-byte groups need whole groups per signal, aligned rows and an order
     // that is a multiple of the group
-    const bool vec = sizeof(T) == 4 && p.T % 4 == 0 && (reinterpret_cast<uintptr_t>(p.in) & 15u) == 0 &&
-                     (reinterpret_cast<uintptr_t>(p.out) & 15u) == 0;
-    if constexpr (sizeof(T) == 4) {
-        if (vec) {
-            // fp32 with whole 16-byte groups: streams staged through shared memory
-            const size_t sm = ti_staged_smem<NP>(kTiThreads, 1);
-            cudaError_t e = cudaFuncSetAttribute(ti_chunk_staged_kernel<NP, REV, false>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(ti_chunk_staged_kernel<NP, REV, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            if (e != cudaSuccess) return e;
-            const unsigned gs = (unsigned)((threads + kTiThreads - 1) / kTiThreads);
-            ti_chunk_staged_kernel<NP, REV, false><<<gs, kTiThreads, sm, st>>>(p);
-            ti_combine_kernel<T, NP, REV><<<(unsigned)((p.B * 32 + 255) / 256), 256, 0, st>>>(p);
-            ti_chunk_staged_kernel<NP, REV, true><<<gs, kTiThreads, sm, st>>>(p);
-            return cudaGetLastError();
-        }
-    }
-    if (vec && NP % 4 == 0)
+    const bool vec = sizeof(T) == 4 && NP % 4 == 0 && p.T % 4 == 0 &&
+                     (reinterpret_cast<uintptr_t>(p.in) & 15u) == 0 && (reinterpret_cast<uintptr_t>(p.out) & 15u) == 0;
+    if (vec)
         ti_chunk_kernel<T, NP, REV, false, true><<<g1, 256, 0, st>>>(p);
     else
         ti_chunk_kernel<T, NP, REV, false, false><<<g1, 256, 0, st>>>(p);
     ti_combine_kernel<T, NP, REV><<<(unsigned)((p.B * 32 + 255) / 256), 256, 0, st>>>(p);
-    if (vec && NP % 4 == 0)
+    if (vec)
         ti_chunk_kernel<T, NP, REV, true, true><<<g1, 256, 0, st>>>(p);
     else
         ti_chunk_kernel<T, NP, REV, true, false><<<g1, 256, 0, st>>>(p);
@@ -665,20 +431,9 @@ cudaError_t launch_grad_a(const T *gx, const T *y, const T *zi, T *ga, int64_t B
     const int64_t nseg = (T_ + seg - 1) / seg;
     const int64_t threads = B * nseg;
     const unsigned grid = (unsigned)((threads + 255) / 256);
-    const bool vec = sizeof(T) == 4 && T_ % 4 == 0 && (reinterpret_cast<uintptr_t>(gx) & 15u) == 0 &&
+    const bool vec = sizeof(T) == 4 && NP % 4 == 0 && T_ % 4 == 0 && (reinterpret_cast<uintptr_t>(gx) & 15u) == 0 &&
                      (reinterpret_cast<uintptr_t>(y) & 15u) == 0;
-    if constexpr (sizeof(T) == 4) {
-        if (vec) {
-            const size_t sm = ti_staged_smem<NP>(kTiGradThreads, 2);
-            const cudaError_t e = cudaFuncSetAttribute(ti_grad_a_staged_kernel<NP>,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            if (e != cudaSuccess) return e;
-            const unsigned gs = (unsigned)((threads + kTiGradThreads - 1) / kTiGradThreads);
-            ti_grad_a_staged_kernel<NP><<<gs, kTiGradThreads, sm, st>>>(gx, y, zi, ga, B, T_, N, seg, nseg, sgn);
-            return cudaGetLastError();
-        }
-    }
-    if (vec && NP % 4 == 0)
+    if (vec)
         ti_grad_a_kernel<T, NP, true><<<grid, 256, 0, st>>>(gx, y, zi, ga, B, T_, N, seg, nseg, sgn);
     else
         ti_grad_a_kernel<T, NP, false><<<grid, 256, 0, st>>>(gx, y, zi, ga, B, T_, N, seg, nseg, sgn);
