@@ -162,13 +162,13 @@ struct Sig {
 };
 
 // Steps per phase-A window (phase D: half of it): orders up to 16 stage 32
-// steps per barrier at two CTAs per SM, larger orders 16+ steps at three
-// (measured on B200: the longer window shortens the backward by ~11 % at
-// order 16 and slows order 24).
+// steps per barrier, larger orders 16+ steps (measured on B200: the longer
+// window shortens the backward by ~11 % at order 16 and slows order 24).
+// Two CTAs per SM up to order 24 (fp32), three above.
 __host__ __device__ constexpr int window_steps(int NP) {
     return (NP <= 16 ? 2 : 1) * NP * ((16 + NP - 1) / NP);
 }
-__host__ __device__ constexpr int ctas_per_sm(int NP, int esz) { return esz == 4 && NP > 16 ? 3 : 2; }
+__host__ __device__ constexpr int ctas_per_sm(int NP, int esz) { return esz == 4 && NP > 24 ? 3 : 2; }
 // Phase-D (exact pass) windows: half the phase-A window, in fix_stages
 // stages (loads issued fix_stages - 1 windows ahead).  Measured on B200 at
 // order 16: quarter-length windows in four stages (the same shared memory)
@@ -598,10 +598,14 @@ __device__ __forceinline__ void map_steps(const T *Ag, const T *xg, unsigned xma
     }
 }
 
-// Filters per phase-A lane: two at orders 8..16, where one 16-byte broadcast
+// Filters per phase-A lane: two at orders 8..24, where one 16-byte broadcast
 // row load per step otherwise feeds a single recurrence and the shared-memory
-// wavefronts (one per coefficient and warp) bound the phase.
-__host__ __device__ constexpr int filters_per_lane(int NP) { return NP >= 8 && NP <= 16 ? 2 : 1; }
+// wavefronts (one per coefficient and warp) bound the phase.  Orders 20 and 24
+// run two CTAs per SM with the full register file (measured on B200 at order
+// 24 against three CTAs of 80 registers with one filter per lane, whose
+// spills dominated: forward 7 %, backward 5 % faster on 64 x 16000, ragged
+// 1024-signal batch 10 % faster).
+__host__ __device__ constexpr int filters_per_lane(int NP) { return NP >= 8 && NP <= 24 ? 2 : 1; }
 
 // Stores the state of filter f of a chunk into an affine map laid out as NP
 // rows of stride rs then z: basis filter f < N is column f of P, the
@@ -651,7 +655,7 @@ __device__ __forceinline__ void fix_steps(const T *Ag, const T *xg, T *og, int j
 // The kernel.
 // ----------------------------------------------------------------------------
 template <typename T, int NP, bool REV, bool NEG>
-__global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 16 ? 2 : 3) chunked_kernel(ChunkParams<T> p) {
+__global__ void __launch_bounds__(Cfg<NP>::THREADS, NP <= 24 ? 2 : 3) chunked_kernel(ChunkParams<T> p) {
     constexpr int W = Cfg<NP>::W;
     constexpr int WD = Cfg<NP>::WD;
     constexpr int DS = Cfg<NP>::DS;
@@ -1268,7 +1272,7 @@ struct Plan {
 
 // Chunks per batch: one group of N+1 lanes per chunk, capped so that the
 // shared memory of a CTA fits the occupancy the kernel is built for
-// (ctas_per_sm: two CTAs per SM up to order 16 and for fp64, three above).
+// (ctas_per_sm: two CTAs per SM up to order 24 and for fp64, three above).
 // `force` > 0 fixes the chunk length (a checkpointed forward and its
 // backward must cut the signal identically).
 inline Plan make_plan(size_t esz, int64_t B, int64_t T, int64_t N, int64_t dflt = 0, int64_t force = 0) {
