@@ -156,11 +156,15 @@ int lpc_b200_backward_checkpointed(int dtype, const void *grad_y, const void *A,
  * into this library (held on every GPU that loads it, until exit).  Returns
  * LPC_ERR_WORKSPACE when the problem needs more scratch than that (roughly
  * 13 to 50 million samples per call at order 16, more for longer signals),
- * LPC_ERR_UNSUPPORTED for orders above 32.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Every call shares the one array: calls whose work overlaps on the GPU
- * (different streams, or several host threads) race and must be serialised
- * by the caller.  Nothing is allocated or freed.
+ * LPC_ERR_UNSUPPORTED for orders above 32.  Every call looks up the array's
+ * device address in the current context (cudaGetSymbolAddress, no
+ * allocation); the first call on a device also loads the module there, so
+ * make that first call before any stream capture.  Every call shares the one
+ * array: calls whose work overlaps on the GPU (different streams, or several
+ * host threads) race and must be serialised by the caller, and changing the
+ * chunk length (lpc_b200_set_chunk_length) while a call is being set up is
+ * unsupported (a plan that outgrows the array returns LPC_ERR_WORKSPACE).
+ * Nothing is allocated or freed.
  * ------------------------------------------------------------------------- */
 int lpc_b200_forward_noalloc(int dtype, const void *x, const void *A,
                              const void *zi, void *y, int64_t B, int64_t T,
